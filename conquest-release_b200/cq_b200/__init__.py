@@ -1,0 +1,317 @@
+"""Python binding of libcqb200.so (B200 block-sparse multiply and LNV solver).
+
+Thin ctypes layer over the C ABI declared in include/cq_b200.h: the product is
+the CUDA library; this module only marshals arguments.  Device arrays are
+passed as torch CUDA tensors (data_ptr) or raw integer device pointers.  There
+is no CPU fallback: importing works without a GPU, but every call that needs
+one raises if the library or the device is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcqb200.so")
+_lib = None
+
+c_int, c_double, c_void_p, c_int64 = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_int64
+P = ctypes.POINTER
+
+# mirror of the status codes in include/cq_b200.h
+CQ_OK, CQ_ERR_ARG, CQ_ERR_OOM, CQ_ERR_CUDA, CQ_ERR_BOUNDS, CQ_ERR_TIMEOUT, CQ_ERR_STATE, CQ_ERR_NOT_CONVERGED = range(8)
+
+
+class LNVParams(ctypes.Structure):
+    """cq_lnv_params (include/cq_b200.h)."""
+    _fields_ = [("n_L_iterations", c_int), ("tolerance", c_double), ("maxpulay", c_int), ("minpulaystep", c_double),
+                ("maxpulaystep", c_double), ("lintol", c_double), ("global_tolerance", c_int), ("vary_mu", c_int),
+                ("invs_max_steps", c_int), ("invs_delta_tol", c_double), ("invs_tol", c_double), ("exact", c_int),
+                ("max_outer", c_int)]
+
+
+class LNVResult(ctypes.Structure):
+    """cq_lnv_result (include/cq_b200.h)."""
+    _fields_ = [("energy", c_double), ("electrons", c_double), ("residual", c_double), ("invs_omega", c_double),
+                ("mcw_sweeps", c_int), ("early_iters", c_int), ("late_iters", c_int), ("ne_corrections", c_int),
+                ("inflexions", c_int), ("converged", c_int), ("n_products", c_int64), ("flops", c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# order of the ranges of the density-matrix chain (cq_lnv_create)
+LNV_RANGE_NAMES = ("S", "H", "L", "T", "LS", "LH", "LSL", "SLS", "TS", "TH", "TL")
+
+
+def lnv_ranges(rs, rh, rl, rt):
+    """Range radii of the chain from the S, H, L and T ranges (src/dimens_module.f90:338-355)."""
+    return {"S": rs, "H": rh, "L": rl, "T": rt, "LS": rl + rs, "LH": rl + rh, "LSL": 2 * rl + rs,
+            "SLS": 2 * rs + rl, "TS": rt + rs, "TH": rt + rh, "TL": rt + rl}
+
+
+class CQError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("cq_b200 error %d: %s" % (code, msg))
+        self.code = code
+
+
+def build():
+    import subprocess
+    subprocess.check_call(["make", "-s", "-C", os.path.join(os.path.dirname(_HERE), "csrc")])
+
+
+def lib():
+    """Load libcqb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise CQError(CQ_ERR_STATE, "libcqb200.so not built: run conquest-release_b200/csrc/Makefile")
+    L = ctypes.CDLL(LIB_PATH)
+    L.cq_last_error.restype = ctypes.c_char_p
+    L.cq_version.restype = ctypes.c_char_p
+    sigs = {
+        "cq_system_create": [c_int, P(c_double), P(c_double), P(c_int), c_int, P(c_double), c_int, c_double, c_double,
+                             P(c_void_p)],
+        "cq_system_destroy": [c_void_p],
+        "cq_range_length": [c_void_p, c_int, P(c_int64), P(c_int64)],
+        "cq_export_index": [c_void_p, c_int, ctypes.c_char_p, P(c_int64), c_int64, P(c_int64)],
+        "cq_export_radius": [c_void_p, c_int, P(c_double), c_int64, P(c_int64)],
+        "cq_mat_mult": [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int],
+        "cq_mat_mult_host": [c_void_p, c_int, c_int, c_int, c_int, P(c_double), P(c_double), P(c_double), c_int],
+        "cq_product_work": [c_void_p, c_int, c_int, c_int, c_int, P(c_int64), P(c_int64)],
+        "cq_matrix_sum": [c_void_p, c_int, c_void_p, c_double, c_int, c_void_p, c_double],
+        "cq_matrix_transpose": [c_void_p, c_int, c_void_p, c_void_p],
+        "cq_matrix_trace": [c_void_p, c_int, c_void_p, P(c_double)],
+        "cq_matrix_product_trace": [c_void_p, c_int, c_void_p, c_void_p, P(c_double)],
+        "cq_synchronize": [c_void_p],
+    }
+    for name, args in sigs.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = c_int
+    lnv_sigs = {
+        "cq_lnv_params_default": [P(LNVParams)],
+        "cq_lnv_create": [c_void_p, P(c_int), c_double, P(LNVParams), P(c_void_p)],
+        "cq_lnv_destroy": [c_void_p],
+        "cq_lnv_set_SH": [c_void_p, c_void_p, c_void_p, c_int],
+        "cq_lnv_invert_S": [c_void_p, P(c_double)],
+        "cq_lnv_find_min_dm": [c_void_p, c_int, P(LNVResult)],
+        "cq_lnv_get": [c_void_p, ctypes.c_char_p, c_void_p, c_int64, c_int],
+        "cq_lnv_put": [c_void_p, ctypes.c_char_p, c_void_p, c_int],
+        "cq_lnv_solve_host": [c_void_p, P(c_double), P(c_double), P(c_double), P(c_double), P(LNVResult)],
+    }
+    for name, args in lnv_sigs.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = c_int
+    ip = P(c_int)
+    kern = [c_int, c_int, ip, ip, ip, ip, ip, ip, P(c_double), P(c_double), P(c_double), ip, ip, ip, ip, ip, ip, ip, ip,
+            c_int, ip, ip, ip, ip, c_int, c_int, c_int, c_int, c_int, c_int]
+    for name in ("cq_m_kern_max", "cq_m_kern_min"):
+        f = getattr(L, name)
+        f.argtypes = kern
+        f.restype = c_int
+    _lib = L
+    return L
+
+
+def check(code):
+    if code != CQ_OK:
+        raise CQError(code, lib().cq_last_error().decode())
+
+
+def _dp(a):
+    return a.ctypes.data_as(P(c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(P(c_int))
+
+
+def _ptr(x):
+    """Device pointer of a torch CUDA tensor or an integer."""
+    if isinstance(x, int):
+        return c_void_p(x)
+    return c_void_p(x.data_ptr())
+
+
+class System:
+    """A periodic system with one block-sparse index per range, resident on the current GPU."""
+
+    def __init__(self, coords, cell, nsf, rcuts, max_atoms_part=34, gap_threshold=14.0, avg_atomic_diameter=5.0):
+        L = lib()
+        coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+        cell = np.ascontiguousarray(cell, dtype=np.float64)
+        nsf = np.ascontiguousarray(nsf, dtype=np.int32)
+        rc = np.ascontiguousarray(rcuts, dtype=np.float64)
+        h = c_void_p()
+        check(L.cq_system_create(coords.shape[0], _dp(coords), _dp(cell), _ip(nsf), len(rc), _dp(rc),
+                                 int(max_atoms_part), float(gap_threshold), float(avg_atomic_diameter), ctypes.byref(h)))
+        self._h = h
+        self.n_atoms = coords.shape[0]
+        self.rcuts = [float(x) for x in rcuts]
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().cq_system_destroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def length(self, r):
+        n, nb = c_int64(), c_int64()
+        check(lib().cq_range_length(self._h, r, ctypes.byref(n), ctypes.byref(nb)))
+        return n.value
+
+    def n_blocks(self, r):
+        n, nb = c_int64(), c_int64()
+        check(lib().cq_range_length(self._h, r, ctypes.byref(n), ctypes.byref(nb)))
+        return nb.value
+
+    def geti(self, name, r=-1):
+        n = c_int64()
+        check(lib().cq_export_index(self._h, r, name.encode(), None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value, dtype=np.int64)
+        check(lib().cq_export_index(self._h, r, name.encode(), out.ctypes.data_as(P(c_int64)), n.value, ctypes.byref(n)))
+        return out
+
+    def radius(self, r):
+        n = c_int64()
+        check(lib().cq_export_radius(self._h, r, None, 0, ctypes.byref(n)))
+        out = np.zeros(n.value)
+        check(lib().cq_export_radius(self._h, r, _dp(out), n.value, ctypes.byref(n)))
+        return out
+
+    # ---- products and algebra on device memory ------------------------------
+    def mat_mult(self, mult_type, ra, rb, rc, a, b, c, exact=True):
+        check(lib().cq_mat_mult(self._h, mult_type, ra, rb, rc, _ptr(a), _ptr(b), _ptr(c), int(bool(exact))))
+
+    def mat_mult_host(self, mult_type, ra, rb, rc, a, b, c, exact=True):
+        for arr in (a, b, c):
+            assert arr.dtype == np.float64 and arr.flags.c_contiguous
+        check(lib().cq_mat_mult_host(self._h, mult_type, ra, rb, rc, _dp(a), _dp(b), _dp(c), int(bool(exact))))
+
+    def product_work(self, mult_type, ra, rb, rc):
+        t, f = c_int64(), c_int64()
+        check(lib().cq_product_work(self._h, mult_type, ra, rb, rc, ctypes.byref(t), ctypes.byref(f)))
+        return t.value, f.value
+
+    def matrix_sum(self, ra, a, alpha, rb, b, beta):
+        check(lib().cq_matrix_sum(self._h, ra, _ptr(a), float(alpha), rb, _ptr(b), float(beta)))
+
+    def transpose(self, r, a, at):
+        check(lib().cq_matrix_transpose(self._h, r, _ptr(a), _ptr(at)))
+
+    def trace(self, r, a):
+        v = c_double()
+        check(lib().cq_matrix_trace(self._h, r, _ptr(a), ctypes.byref(v)))
+        return v.value
+
+    def product_trace(self, r, a, b):
+        v = c_double()
+        check(lib().cq_matrix_product_trace(self._h, r, _ptr(a), _ptr(b), ctypes.byref(v)))
+        return v.value
+
+    def synchronize(self):
+        check(lib().cq_synchronize(self._h))
+
+
+def m_kern(kind, k_off, kpart, ib_nd_acc, ibaddr, nbnab, ibpart, ibseq, bndim2, a, b, c, ahalo, chalo, at,
+           mx_absb=0, mx_part=0, mx_iprim=0):
+    """Call cq_m_kern_max (kind='max') or cq_m_kern_min (kind='min') with Fortran-style int32 arrays.
+
+    ahalo = dict(nh_part, j_beg, j_seq, ndimi, ndimj); chalo = dict(i_halo, i_hbeg, i_h2d, ni_in_halo);
+    at = dict(i_prim, i_beg, i_nd_beg, n_hnab).  a, b, c are float64 numpy arrays (updated in place).
+    """
+    I = lambda x: np.ascontiguousarray(x, dtype=np.int32)
+    arrs = [I(ib_nd_acc), I(ibaddr), I(nbnab), I(ibpart), I(ibseq), I(bndim2)]
+    ah = [I(ahalo[k]) for k in ("nh_part", "j_beg", "j_seq", "ndimi", "ndimj")]
+    ch = [I(chalo[k]) for k in ("i_halo", "i_hbeg", "i_h2d")]
+    tr = [I(at[k]) for k in ("i_prim", "i_beg", "i_nd_beg", "n_hnab")]
+    f = lib().cq_m_kern_max if kind == "max" else lib().cq_m_kern_min
+    check(f(int(k_off), int(kpart), *[_ip(x) for x in arrs], _dp(a), _dp(b), _dp(c), *[_ip(x) for x in ah],
+            *[_ip(x) for x in ch], int(chalo["ni_in_halo"]), *[_ip(x) for x in tr], int(mx_absb), int(mx_part),
+            int(mx_iprim), a.size, b.size, c.size))
+
+
+def lnv_params(**kw):
+    p = LNVParams()
+    check(lib().cq_lnv_params_default(ctypes.byref(p)))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+class LNV:
+    """Density-matrix solver on a System whose ranges include those of the chain.
+
+    `range_ids` maps each name of LNV_RANGE_NAMES to a range index of the system.
+    """
+
+    def __init__(self, system, range_ids, ne_spin, **params):
+        self.system = system
+        ids = (c_int * 11)(*[int(range_ids[n]) for n in LNV_RANGE_NAMES])
+        self._p = lnv_params(**params)
+        h = c_void_p()
+        check(lib().cq_lnv_create(system.handle, ids, float(ne_spin), ctypes.byref(self._p), ctypes.byref(h)))
+        self._h = h
+        self.range_ids = dict(range_ids)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().cq_lnv_destroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_SH(self, S, H):
+        if isinstance(S, np.ndarray):
+            S = np.ascontiguousarray(S, np.float64); H = np.ascontiguousarray(H, np.float64)
+            check(lib().cq_lnv_set_SH(self._h, S.ctypes.data_as(c_void_p), H.ctypes.data_as(c_void_p), 0))
+        else:
+            check(lib().cq_lnv_set_SH(self._h, _ptr(S), _ptr(H), 1))
+
+    def invert_S(self):
+        w = c_double()
+        check(lib().cq_lnv_invert_S(self._h, ctypes.byref(w)))
+        return w.value
+
+    def find_min_dm(self, resetL=True):
+        r = LNVResult()
+        check(lib().cq_lnv_find_min_dm(self._h, int(bool(resetL)), ctypes.byref(r)))
+        return r.as_dict()
+
+    def get(self, name):
+        n = self.system.length(self.range_ids[{"L": "L", "K": "H", "T": "T", "S": "S", "H": "H", "phi": "L"}[name]])
+        out = np.zeros(n)
+        check(lib().cq_lnv_get(self._h, name.encode(), out.ctypes.data_as(c_void_p), n, 0))
+        return out
+
+    def put(self, name, arr):
+        arr = np.ascontiguousarray(arr, np.float64)
+        check(lib().cq_lnv_put(self._h, name.encode(), arr.ctypes.data_as(c_void_p), 0))
+
+    def solve_host(self, S, H, want_L=False, want_K=False):
+        S = np.ascontiguousarray(S, np.float64); H = np.ascontiguousarray(H, np.float64)
+        Lo = np.zeros(self.system.length(self.range_ids["L"])) if want_L else None
+        Ko = np.zeros(self.system.length(self.range_ids["H"])) if want_K else None
+        r = LNVResult()
+        check(lib().cq_lnv_solve_host(self._h, _dp(S), _dp(H), _dp(Lo) if Lo is not None else None,
+                                      _dp(Ko) if Ko is not None else None, ctypes.byref(r)))
+        return r.as_dict(), Lo, Ko

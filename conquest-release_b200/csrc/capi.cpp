@@ -1,0 +1,325 @@
+// C ABI of libcqb200.so (declarations and reference citations in include/cq_b200.h).
+#include <algorithm>
+#include <cstring>
+#include <functional>
+#include <numeric>
+#include <string>
+
+#include "cq_internal.hpp"
+
+namespace cqb {
+
+static thread_local std::string g_last_error = "";
+void set_last_error(const std::string& m) { g_last_error = m; }
+
+System::~System() {
+  plans.clear();
+  addmaps.clear();
+  ranges.clear();
+  if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+// drop-in kernels (one m_kern_max / m_kern_min call): explicit offsets prepared on the host
+void launch_dropin(int type, const int64_t* d_out, const int* d_dims, const int64_t* d_ptr, const int64_t* d_pairs,
+                   int n_out, const double* x, const double* b, double* out, cudaStream_t st);
+
+}  // namespace cqb
+
+using namespace cqb;
+
+struct cq_system {
+  cqb::System S;
+  // staging buffers of the host-memory entry points
+  DevBuf<double> ha, hb, hc;
+};
+
+template <class F>
+static int guarded(F&& f) {
+  try {
+    f();
+    return CQ_OK;
+  } catch (const cqb::Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host allocation failed");
+    return CQ_ERR_OOM;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return CQ_ERR_STATE;
+  }
+}
+
+namespace cqb {
+System& system_of(cq_system* s) {
+  CQ_CHECK(s != nullptr, CQ_ERR_ARG, "null system");
+  return s->S;
+}
+int guarded_call(const std::function<void()>& f) { return guarded(f); }
+}  // namespace cqb
+
+static void check_sys(cq_system* s) { CQ_CHECK(s != nullptr, CQ_ERR_ARG, "null system"); }
+static void check_range(cq_system* s, int r) {
+  CQ_CHECK(r >= 0 && r < (int)s->S.ranges.size(), CQ_ERR_ARG, "range index out of bounds");
+}
+
+extern "C" {
+
+const char* cq_last_error(void) { return g_last_error.c_str(); }
+const char* cq_version(void) { return "cqb200 0.1 (sm_100a)"; }
+
+int cq_system_create(int n_atoms, const double* coords, const double* cell, const int* nsf, int n_ranges,
+                     const double* rcuts, int max_atoms_part, double gap_threshold, double avg_atomic_diameter,
+                     cq_system** out) {
+  return guarded([&] {
+    CQ_CHECK(out && coords && cell && nsf && rcuts && n_ranges > 0, CQ_ERR_ARG, "null argument");
+    *out = nullptr;
+    for (int r = 0; r < n_ranges; ++r) CQ_CHECK(rcuts[r] > 0, CQ_ERR_ARG, "ranges must be positive");
+    for (int i = 0; i < n_atoms; ++i) CQ_CHECK(nsf[i] >= 1 && nsf[i] <= 16, CQ_ERR_ARG, "block sizes must be 1..16");
+    auto sys = std::make_unique<cq_system>();
+    System& S = sys->S;
+    CQ_CUDA(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
+    S.own_stream = true;
+    GeometryParams prm;
+    prm.max_atoms_part = max_atoms_part > 0 ? max_atoms_part : 34;
+    prm.gap_threshold = gap_threshold;
+    prm.avg_atomic_diameter = avg_atomic_diameter > 0 ? avg_atomic_diameter : 5.0;
+    double rmax = *std::max_element(rcuts, rcuts + n_ranges);
+    build_geometry(S.geo, n_atoms, coords, cell, nsf, rmax, prm);
+    upload_geometry(S);
+    for (int r = 0; r < n_ranges; ++r) {
+      S.ranges.emplace_back(new RangeIndex());
+      S.ranges.back()->rcut = rcuts[r];
+      build_range_index(S, *S.ranges.back());
+    }
+    CQ_CUDA(cudaStreamSynchronize(S.stream));
+    *out = sys.release();
+  });
+}
+
+int cq_system_destroy(cq_system* sys) {
+  return guarded([&] {
+    if (sys) {
+      cudaStreamSynchronize(sys->S.stream);
+      delete sys;
+    }
+  });
+}
+
+int cq_range_length(cq_system* sys, int r, int64_t* length, int64_t* n_blocks) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, r);
+    if (length) *length = sys->S.ranges[r]->length;
+    if (n_blocks) *n_blocks = sys->S.ranges[r]->nnz;
+  });
+}
+
+int cq_export_index(cq_system* sys, int r, const char* name, int64_t* out, int64_t cap, int64_t* n) {
+  return guarded([&] {
+    check_sys(sys);
+    CQ_CHECK(name && n, CQ_ERR_ARG, "null argument");
+    std::vector<int64_t> v;
+    export_range_array(sys->S, r, name, v);
+    *n = (int64_t)v.size();
+    if (out) std::memcpy(out, v.data(), sizeof(int64_t) * std::min<int64_t>(cap, (int64_t)v.size()));
+  });
+}
+
+int cq_export_radius(cq_system* sys, int r, double* out, int64_t cap, int64_t* n) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, r);
+    CQ_CHECK(n, CQ_ERR_ARG, "null argument");
+    RangeIndex& R = *sys->S.ranges[r];
+    *n = R.nnz;
+    if (out) {
+      std::vector<double> v = R.nb_radius.download(sys->S.stream);
+      std::memcpy(out, v.data(), sizeof(double) * std::min<int64_t>(cap, R.nnz));
+    }
+  });
+}
+
+int cq_mat_mult(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a_dev, const double* b_dev, double* c_dev,
+                int exact) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, ra); check_range(sys, rb); check_range(sys, rc);
+    CQ_CHECK(a_dev && b_dev && c_dev, CQ_ERR_ARG, "null operand");
+    ProductPlan& P = get_plan(sys->S, mult_type, ra, rb, rc);
+    launch_mat_mult(sys->S, P, a_dev, b_dev, c_dev, exact);
+  });
+}
+
+int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c,
+                     int exact) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, ra); check_range(sys, rb); check_range(sys, rc);
+    CQ_CHECK(a && b && c, CQ_ERR_ARG, "null operand");
+    System& S = sys->S;
+    int64_t la = S.ranges[ra]->length, lb = S.ranges[rb]->length, lc = S.ranges[rc]->length;
+    if (sys->ha.n < (size_t)std::max<int64_t>(la, 1)) sys->ha.alloc(std::max<int64_t>(la, 1));
+    if (sys->hb.n < (size_t)std::max<int64_t>(lb, 1)) sys->hb.alloc(std::max<int64_t>(lb, 1));
+    if (sys->hc.n < (size_t)std::max<int64_t>(lc, 1)) sys->hc.alloc(std::max<int64_t>(lc, 1));
+    ProductPlan& P = get_plan(S, mult_type, ra, rb, rc);
+    if (mult_type == 1) CQ_CUDA(cudaMemcpyAsync(sys->ha.p, a, la * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+    CQ_CUDA(cudaMemcpyAsync(sys->hb.p, b, lb * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+    if (mult_type == 2) CQ_CUDA(cudaMemcpyAsync(sys->hc.p, c, lc * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+    launch_mat_mult(S, P, sys->ha.p, sys->hb.p, sys->hc.p, exact);
+    if (mult_type == 1) CQ_CUDA(cudaMemcpyAsync(c, sys->hc.p, lc * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+    else CQ_CUDA(cudaMemcpyAsync(a, sys->ha.p, la * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+    CQ_CUDA(cudaStreamSynchronize(S.stream));
+  });
+}
+
+int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* triples, int64_t* flops) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, ra); check_range(sys, rb); check_range(sys, rc);
+    ProductPlan& P = get_plan(sys->S, mult_type, ra, rb, rc);
+    if (triples) *triples = P.n_pairs;
+    if (flops) *flops = P.flops;
+  });
+}
+
+int cq_matrix_sum(cq_system* sys, int ra, double* a_dev, double alpha, int rb, const double* b_dev, double beta) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, ra); check_range(sys, rb);
+    System& S = sys->S;
+    if (ra == rb) {
+      dev_scale(S, a_dev, S.ranges[ra]->length, alpha);
+      dev_axpy(S, a_dev, S.ranges[ra]->length, beta, b_dev);
+    } else {
+      dev_matrix_add(S, ra, a_dev, alpha, rb, b_dev, beta);
+    }
+  });
+}
+
+int cq_matrix_transpose(cq_system* sys, int r, const double* a_dev, double* at_dev) {
+  return guarded([&] { check_sys(sys); check_range(sys, r); dev_transpose(sys->S, r, a_dev, at_dev); });
+}
+
+int cq_matrix_trace(cq_system* sys, int r, const double* a_dev, double* result) {
+  return guarded([&] { check_sys(sys); check_range(sys, r); *result = dev_trace(sys->S, r, a_dev); });
+}
+
+int cq_matrix_product_trace(cq_system* sys, int r, const double* a_dev, const double* b_dev, double* result) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, r);
+    *result = dev_dot(sys->S, a_dev, b_dev, sys->S.ranges[r]->length);
+  });
+}
+
+int cq_synchronize(cq_system* sys) {
+  return guarded([&] { check_sys(sys); CQ_CUDA(cudaStreamSynchronize(sys->S.stream)); });
+}
+
+// ---------------------------------------------------------------------------
+// drop-in m_kern_max / m_kern_min: the loop nest of the default kernel walked
+// on the host to list the block triples of this partition (in order), the
+// arithmetic done on the GPU with the same per-element operation sequence.
+// ---------------------------------------------------------------------------
+static int dropin(int type, int k_off, int kpart, const int* ib_nd_acc, const int* ibaddr, const int* nbnab,
+                  const int* ibpart, const int* ibseq, const int* bndim2, double* a, const double* b, double* c,
+                  const int* nh_part, const int* j_beg, const int* j_seq, const int* ndimi, const int* ndimj,
+                  const int* i_halo, const int* i_hbeg, const int* i_h2d, int ni_in_halo, const int* i_prim,
+                  const int* i_beg, const int* i_nd_beg, const int* n_hnab, int lena, int lenb, int lenc) {
+  return guarded([&] {
+    CQ_CHECK(ib_nd_acc && ibaddr && nbnab && ibpart && ibseq && bndim2 && a && b && c && nh_part && j_beg && j_seq &&
+                 ndimi && ndimj && i_halo && i_hbeg && i_h2d && i_prim && i_beg && i_nd_beg && n_hnab,
+             CQ_ERR_ARG, "null argument");
+    CQ_CHECK(kpart >= 1, CQ_ERR_ARG, "kpart must be >= 1");
+    // Fortran 1-based views
+    auto F = [](const int* p) { return p - 1; };
+    const int *ib_nd_acc1 = F(ib_nd_acc), *ibaddr1 = F(ibaddr), *nbnab1 = F(nbnab), *ibpart1 = F(ibpart),
+              *ibseq1 = F(ibseq), *bndim21 = F(bndim2), *nh_part1 = F(nh_part), *j_beg1 = F(j_beg), *j_seq1 = F(j_seq),
+              *ndimi1 = F(ndimi), *ndimj1 = F(ndimj), *i_halo1 = F(i_halo), *i_hbeg1 = F(i_hbeg), *i_h2d1 = F(i_h2d),
+              *i_prim1 = F(i_prim), *i_beg1 = F(i_beg), *i_nd_beg1 = F(i_nd_beg), *n_hnab1 = F(n_hnab);
+    // triples (out_off, x_off, b_off, nd_out_rows, nd_out_cols, ndk) in kernel order, 0-based element offsets
+    struct Tri { int64_t out, x, b; int r, cols, kd; };
+    std::vector<Tri> tri;
+    std::vector<int> jb2ch;
+    for (int k = 1; k <= nh_part1[kpart]; ++k) {
+      int k_in_halo = j_beg1[kpart] + k - 1;
+      int k_in_part = j_seq1[k_in_halo];
+      int nbkbeg = ibaddr1[k_in_part];
+      int nb_nd_kbeg = ib_nd_acc1[k_in_part];
+      int nd3 = ndimj1[k_in_halo];
+      int nbn = nbnab1[k_in_part];
+      jb2ch.assign(nbn + 1, 0);
+      for (int j = 1; j <= nbn; ++j)
+        jb2ch[j] = i_halo1[i_hbeg1[ibpart1[nbkbeg + j - 1] + k_off] + ibseq1[nbkbeg + j - 1] - 1];
+      int nabeg = i_nd_beg1[k_in_halo];
+      for (int i = 1; i <= n_hnab1[k_in_halo]; ++i) {
+        int ip = i_prim1[i_beg1[k_in_halo] + i - 1];
+        int nd1 = ndimi1[ip];
+        int64_t icad = (int64_t)(ip - 1) * ni_in_halo;
+        int nbbeg = nb_nd_kbeg;
+        for (int j = 1; j <= nbn; ++j) {
+          int nd2 = bndim21[nbkbeg + j - 1];
+          if (jb2ch[j] != 0) {
+            int ncbeg = i_h2d1[icad + jb2ch[j]];
+            if (ncbeg != 0) {
+              CQ_CHECK(nabeg + nd1 * nd3 - 1 <= lena && nbbeg + nd3 * nd2 - 1 <= lenb && ncbeg + nd1 * nd2 - 1 <= lenc,
+                       CQ_ERR_BOUNDS, "m_kern: block outside the passed arrays");
+              if (type == 1) tri.push_back({ncbeg - 1, nabeg - 1, nbbeg - 1, nd1, nd2, nd3});
+              else tri.push_back({nabeg - 1, ncbeg - 1, nbbeg - 1, nd1, nd3, nd2});
+            }
+          }
+          nbbeg += nd3 * nd2;
+        }
+        nabeg += nd1 * nd3;
+      }
+    }
+    if (tri.empty()) return;
+    // group by output block, preserving order
+    std::vector<int> order(tri.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int p, int q) { return tri[p].out < tri[q].out; });
+    std::vector<int64_t> out_off, ptr, pairs;
+    std::vector<int> dims;
+    for (size_t t = 0; t < order.size(); ++t) {
+      const Tri& T = tri[order[t]];
+      if (t == 0 || T.out != tri[order[t - 1]].out) {
+        out_off.push_back(T.out);
+        dims.push_back(T.r); dims.push_back(T.cols);
+        ptr.push_back((int64_t)t);
+      }
+      pairs.push_back(T.x); pairs.push_back(T.b); pairs.push_back(T.kd);
+    }
+    ptr.push_back((int64_t)order.size());
+    cudaStream_t st = 0;
+    DevBuf<int64_t> d_out, d_ptr, d_pairs;
+    DevBuf<int> d_dims;
+    DevBuf<double> da, db, dc;
+    d_out.upload(out_off, st); d_ptr.upload(ptr, st); d_pairs.upload(pairs, st); d_dims.upload(dims, st);
+    da.upload(a, lena, st); db.upload(b, lenb, st); dc.upload(c, lenc, st);
+    if (type == 1) launch_dropin(1, d_out.p, d_dims.p, d_ptr.p, d_pairs.p, (int)out_off.size(), da.p, db.p, dc.p, st);
+    else launch_dropin(2, d_out.p, d_dims.p, d_ptr.p, d_pairs.p, (int)out_off.size(), dc.p, db.p, da.p, st);
+    if (type == 1) CQ_CUDA(cudaMemcpyAsync(c, dc.p, sizeof(double) * lenc, cudaMemcpyDeviceToHost, st));
+    else CQ_CUDA(cudaMemcpyAsync(a, da.p, sizeof(double) * lena, cudaMemcpyDeviceToHost, st));
+    CQ_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int cq_m_kern_max(int k_off, int kpart, const int* ib_nd_acc, const int* ibaddr, const int* nbnab, const int* ibpart,
+                  const int* ibseq, const int* bndim2, const double* a, const double* b, double* c,
+                  const int* ahalo_nh_part, const int* ahalo_j_beg, const int* ahalo_j_seq, const int* ahalo_ndimi,
+                  const int* ahalo_ndimj, const int* chalo_i_halo, const int* chalo_i_hbeg, const int* chalo_i_h2d,
+                  int chalo_ni_in_halo, const int* at_i_prim, const int* at_i_beg, const int* at_i_nd_beg,
+                  const int* at_n_hnab, int mx_absb, int mx_part, int mx_iprim, int lena, int lenb, int lenc) {
+  (void)mx_absb; (void)mx_part; (void)mx_iprim;
+  return dropin(1, k_off, kpart, ib_nd_acc, ibaddr, nbnab, ibpart, ibseq, bndim2, const_cast<double*>(a), b, c,
+                ahalo_nh_part, ahalo_j_beg, ahalo_j_seq, ahalo_ndimi, ahalo_ndimj, chalo_i_halo, chalo_i_hbeg,
+                chalo_i_h2d, chalo_ni_in_halo, at_i_prim, at_i_beg, at_i_nd_beg, at_n_hnab, lena, lenb, lenc);
+}
+
+int cq_m_kern_min(int k_off, int kpart, const int* ib_nd_acc, const int* ibaddr, const int* nbnab, const int* ibpart,
+                  const int* ibseq, const int* bndim2, double* a, const double* b, const double* c,
+                  const int* ahalo_nh_part, const int* ahalo_j_beg, const int* ahalo_j_seq, const int* ahalo_ndimi,
+                  const int* ahalo_ndimj, const int* chalo_i_halo, const int* chalo_i_hbeg, const int* chalo_i_h2d,
+                  int chalo_ni_in_halo, const int* at_i_prim, const int* at_i_beg, const int* at_i_nd_beg,
+                  const int* at_n_hnab, int mx_absb, int mx_part, int mx_iprim, int lena, int lenb, int lenc) {
+  (void)mx_absb; (void)mx_part; (void)mx_iprim;
+  return dropin(2, k_off, kpart, ib_nd_acc, ibaddr, nbnab, ibpart, ibseq, bndim2, a, b, const_cast<double*>(c),
+                ahalo_nh_part, ahalo_j_beg, ahalo_j_seq, ahalo_ndimi, ahalo_ndimj, chalo_i_halo, chalo_i_hbeg,
+                chalo_i_h2d, chalo_ni_in_halo, at_i_prim, at_i_beg, at_i_nd_beg, at_n_hnab, lena, lenb, lenc);
+}
+
+}  // extern "C"

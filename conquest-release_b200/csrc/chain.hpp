@@ -1,0 +1,100 @@
+// LNV / McWeeny solver state (see chain.cpp).
+#pragma once
+#include <vector>
+
+#include "cq_internal.hpp"
+
+namespace cqb {
+
+class LNVSolver;
+
+// a device block matrix of one named range; temporaries return to their pool on destruction
+struct DMat {
+  int rng = -1;
+  double* p = nullptr;
+  int64_t n = 0;
+  LNVSolver* owner = nullptr;
+  DMat() = default;
+  DMat(int r, double* ptr, int64_t len, LNVSolver* o) : rng(r), p(ptr), n(len), owner(o) {}
+  DMat(const DMat&) = delete;
+  DMat& operator=(const DMat&) = delete;
+  DMat(DMat&& o) noexcept : rng(o.rng), p(o.p), n(o.n), owner(o.owner) { o.p = nullptr; o.owner = nullptr; }
+  DMat& operator=(DMat&& o) noexcept {
+    if (this != &o) {
+      this->~DMat();
+      rng = o.rng; p = o.p; n = o.n; owner = o.owner;
+      o.p = nullptr; o.owner = nullptr;
+    }
+    return *this;
+  }
+  ~DMat();
+};
+
+bool sym_inverse_bk(double* A, int n);
+
+struct LNVStats {
+  int64_t n_products = 0, flops = 0, n_reductions = 0, n_lnv = 0;
+  int mcw_sweeps = 0, early_iters = 0, late_iters = 0, ne_corrections = 0, inflexions = 0, converged = 0;
+  double energy = 0, electrons = 0, last_energy = 0, last_residual = 0, invs_omega = 0;
+  double mubar = 0, lambda = 0, hmin = 0, hmax = 0;
+};
+
+class LNVSolver {
+ public:
+  // named ranges of the chain, in the order of cq_lnv_create's range list
+  enum Rng { RS = 0, RH, RL, RT, RLS, RLH, RLSL, RSLS, RTS, RTH, RTL, NR };
+  enum MultId { L_S_LS = 0, L_H_LH, T_S_TS, SL_S_SLS, LS_L_LSL, HL_S_LSL, HLS_LS_L, SLS_LS_L, LSL_SL_H, TS_T_T,
+                TH_T_L, T_H_TH, T_L_TL, TL_T_L };
+  struct Mult { int type, a, b, c; };
+  static const Mult kMults[];
+
+  LNVSolver(System& sys, const int ranges[NR], double ne_spin, const cq_lnv_params& p);
+
+  System& S;
+  cq_lnv_params prm;
+  int R[NR];
+  double ne, n_o;
+  int ni_in_cell;
+  double delta_e = 0.0;  // `save` variable of FindMinDM
+  LNVStats stats;
+  DMat Smat, Hmat, L, T, Ttran, LS, SL, K, phi;
+
+  DMat temp(int rng);
+  void release(DMat& m);
+
+  double invert_S();
+  void find_min_dm(bool resetL);
+  void lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim, double* electrons, double* energy);
+
+ private:
+  std::vector<DevBuf<double>> owned_;
+  std::vector<DevBuf<double>> pool_;
+  std::map<int, std::vector<double*>> free_;
+  DMat own(int rng);
+
+  void product(const DMat& A, const DMat& B, DMat& C, MultId id);
+  void mult_dispatch(ProductPlan& P, double* a, const double* b, double* c);
+  void msum(double alpha, DMat& A, double beta, const DMat& B);
+  void scale(double alpha, DMat& A);
+  void transpose(const DMat& A, DMat& AT);
+  double ptrace(const DMat& A, const DMat& B);
+  double trace(const DMat& A);
+  void copy(DMat& dst, const DMat& src);
+  void set_identity_onsite(DMat& A);
+  void symmetrise_L();
+  void tmt(const DMat& M, DMat& out, DMat& tl, const DMat& Tright);
+  double gnorm(const DMat& A, const DMat& B);
+  void init_mcw();
+  void mcw_mm_nonds(DMat& RhoNew, double& energy, double& c);
+  double mcw_min(int n_L_iterations);
+  static double solve_cubic(double a, double b, double c, double guess);
+  void correct_electron_number();
+  bool line_min_L(DMat& M3, DMat& D, DMat& mtemp, DMat& SM3, double energy_in, double& energy_out, double& zeta);
+  void project_search(DMat& search, DMat& SM3, DMat& Sphi, DMat& mtemp);
+  void project_gradient(DMat& M3, DMat& SM3, DMat& Sphi, DMat& mtemp);
+  int early_dm(int ndone, bool& inflex);
+  int late_dm(int ndone, bool& done, double& deltaE);
+  static void do_pulay(int iPulay, const double* Aij, int n, int max_n, double* al);
+};
+
+}  // namespace cqb

@@ -1,0 +1,218 @@
+// Internal declarations of the B200 block-sparse multiply / LNV library.
+// Everything here is device-resident state plus the host-side geometry that
+// feeds the GPU index builders.  See include/cq_b200.h for the public C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/cq_b200.h"
+
+namespace cqb {
+
+// ---------------------------------------------------------------------------
+// errors: every failure becomes a status code at the C ABI
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+void set_last_error(const std::string& m);
+
+#define CQ_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      throw ::cqb::Error(CQ_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+  } while (0)
+#define CQ_CHECK(cond, code, msg)                 \
+  do {                                            \
+    if (!(cond)) throw ::cqb::Error(code, (msg)); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// device buffer (RAII, stream-ordered allocator)
+// ---------------------------------------------------------------------------
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) {
+      cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+      if (e != cudaSuccess) { p = nullptr; n = 0; throw Error(CQ_ERR_OOM, "cudaMalloc failed: " + std::string(cudaGetErrorString(e))); }
+    }
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr; n = 0;
+  }
+  void upload(const T* h, size_t count, cudaStream_t s) {
+    alloc(count);
+    if (count) CQ_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
+  std::vector<T> download(cudaStream_t s) const {
+    std::vector<T> v(n);
+    if (n) {
+      CQ_CUDA(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+      CQ_CUDA(cudaStreamSynchronize(s));
+    }
+    return v;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// host geometry: partitions, primary set, covering set (one process)
+// All indices 0-based; partition/cover labels keep the reference's 1-based
+// CC numbering where they enter index arithmetic.
+// ---------------------------------------------------------------------------
+struct Geometry {
+  int n_atoms = 0;
+  double cell[3] = {0, 0, 0};
+  std::vector<double> coord;          // wrapped, input order, 3*n
+  std::vector<int> nsf;               // block size per input atom
+  int n_parts[3] = {1, 1, 1};
+  int np_in_cell = 0;
+  std::vector<int> hilbert_to_cc;     // [hilbert pos] -> 1-based CC label
+  std::vector<int> cc_to_seq;         // [cc label] -> 0-based primary-partition position
+  std::vector<int> part_natoms;       // [cc label]
+  std::vector<int> part_first_cell;   // [cc label] first cell-order atom (0-based)
+  std::vector<int> cell_to_global;    // cell-order -> input atom
+  // primary set (primary order == cell order on one process)
+  int n_prim = 0;
+  std::vector<int> prim_global;       // [p] input atom
+  std::vector<int> prim_part;         // [p] primary partition position
+  std::vector<int> prim_seq;          // [p] 1-based sequence in partition
+  std::vector<int> part_first_prim;   // [partition position] first primary atom
+  std::vector<int> part_disp;         // [partition position*3] idisp_prim
+  std::vector<int> prim_cover_label;  // [p] lab_cover of its partition (1-based)
+  std::vector<double> prim_x;         // [3p]
+  // covering set
+  int ncover[3] = {0, 0, 0};
+  int nspan[3] = {0, 0, 0};
+  int ng_cover = 0, n_cover_atoms = 0;
+  std::vector<int> cover_label;       // [np] 1-based lab_cover
+  std::vector<int> cover_cell;        // [np] 1-based lab_cell (CC of the home partition)
+  std::vector<int> cover_first;       // [np] first cover atom (0-based)
+  std::vector<int> cover_count;       // [np]
+  std::vector<int> label_to_cover;    // [label] -> np (0-based), -1 if none
+  std::vector<double> cover_x;        // [3c]
+  std::vector<int> cover_global;      // [c] input atom
+  std::vector<int> cover_part;        // [c] cover partition np
+  std::vector<int> cover_seq;         // [c] 1-based seq in partition
+  std::vector<int> cover_nsf;         // [c]
+  std::vector<int> cover_home_prim;   // [c] primary atom of the same input atom
+  std::vector<int> global_to_prim;    // [input atom] -> primary index
+};
+
+struct GeometryParams {
+  int max_atoms_part = 34;
+  double gap_threshold = 14.0;
+  double avg_atomic_diameter = 5.0;
+};
+
+void build_geometry(Geometry& g, int n, const double* coords, const double* cell, const int* nsf, double cover_rcut,
+                    const GeometryParams& prm);
+
+// ---------------------------------------------------------------------------
+// device geometry + one index per range
+// ---------------------------------------------------------------------------
+struct DevGeometry {
+  DevBuf<double> prim_x, cover_x;
+  DevBuf<int> prim_nsf, prim_cover_label, prim_seq, prim_part, part_disp, cover_nsf, cover_part, cover_seq,
+      cover_label_of_part, label_to_cover, cover_first, cover_home_prim, part_first_prim;
+};
+
+struct RangeIndex {
+  double rcut = 0;
+  int nnz = 0;                  // stored blocks
+  int64_t length = 0;           // stored elements
+  int ni_in_halo = 0, np_in_halo = 0;
+  int max_row = 0;              // largest neighbour count of a row
+  DevBuf<int> row_ptr;          // [n_prim+1]
+  DevBuf<int64_t> row_elem;     // [n_prim+1]
+  DevBuf<int> nb_cover;         // [nnz] cover atom (row-sorted ascending)
+  DevBuf<int> nb_halo;          // [nnz] halo index
+  DevBuf<int64_t> nb_elem;      // [nnz] first element of the block
+  DevBuf<int> nb_row;           // [nnz] owning primary atom
+  DevBuf<int> nb_ibpart;        // [nnz] partition displacement code (end_part_comms)
+  DevBuf<double> nb_radius;     // [nnz]
+  DevBuf<int64_t> onsite;       // [n_prim] element offset of the self block
+  DevBuf<int> cover_to_halo;    // [n_cover_atoms] -> halo index or -1
+  DevBuf<int> halo_cover;       // [ni_in_halo]
+  DevBuf<int> col_ptr;          // [ni_in_halo+1] retro lists (primary atoms of each halo atom)
+  DevBuf<int> col_row;          // [nnz]
+  DevBuf<int> col_blk;          // [nnz]
+  DevBuf<int> trans_dest;       // [nnz] block of the global transpose
+  std::vector<int> h_row_ptr;   // host copy (small)
+};
+
+// Per-product pair lists: for each output block, the ordered list of
+// (first operand block, B block) pairs in the reference's summation order.
+struct ProductPlan {
+  int mult_type = 1;
+  int ra = -1, rb = -1, rc = -1;  // mat_mult roles: a (A or type-2 output), b, c (C or type-2 input)
+  int out_range = -1;             // range of the block list owner (C for type 1, a for type 2)
+  int64_t n_pairs = 0;            // total (x, b) pairs = block triples with a stored result
+  int64_t flops = 0;              // 2 * sum nd_i nd_j nd_k over the triples
+  DevBuf<int64_t> ptr;            // [n_out_blocks+1]
+  DevBuf<int2> pairs;             // [n_pairs] (x block, b block)
+};
+
+struct AddMap {                   // partner of each block of range A in range B (-1 = none)
+  DevBuf<int> partner;
+};
+
+struct System {
+  Geometry geo;
+  DevGeometry dg;
+  std::vector<std::unique_ptr<RangeIndex>> ranges;
+  std::map<std::tuple<int, int, int, int>, std::unique_ptr<ProductPlan>> plans;
+  std::map<std::pair<int, int>, std::unique_ptr<AddMap>> addmaps;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int uniform_nsf = 0;            // block size when every atom has the same one, else 0
+  DevBuf<double> red_scratch;     // partial sums of the deterministic reductions
+  ~System();
+};
+
+// index.cu
+void upload_geometry(System& S);
+void build_range_index(System& S, RangeIndex& R);
+ProductPlan& get_plan(System& S, int mult_type, int ra, int rb, int rc);
+AddMap& get_addmap(System& S, int ra, int rb);
+void export_range_array(System& S, int r, const std::string& name, std::vector<int64_t>& out);
+
+// mult.cu
+void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, double* c, int exact);
+
+// algebra.cu
+void dev_scale(System& S, double* a, int64_t n, double alpha);
+void dev_axpy(System& S, double* a, int64_t n, double beta, const double* b);
+void dev_copy(System& S, double* dst, const double* src, int64_t n);
+void dev_matrix_add(System& S, int ra, double* a, double alpha, int rb, const double* b, double beta);
+void dev_transpose(System& S, int r, const double* a, double* at);
+double dev_dot(System& S, const double* x, const double* y, int64_t n);
+double dev_trace(System& S, int r, const double* a);
+void dev_h_limits(System& S, int r, const double* h, double* hmin, double* hmax);
+
+}  // namespace cqb

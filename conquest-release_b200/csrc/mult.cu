@@ -1,0 +1,215 @@
+// FP64 block-sparse products on the pair lists built in index.cu.
+//
+// Output stationary: each output block is owned by one group of lanes (one
+// lane per element) that walks the block's (operand, B) pair list in the
+// reference's order, so every element sees exactly the operation sequence of
+// the default kernel (src/multiply_kernel_default.f90:204-214 for type 1,
+// 390-402 for type 2):
+//   type 1  c(n1,n2) = sum over k (A-halo order) of sum_n3 a(n1,n3) * b(n3,n2)
+//   type 2  a(n1,n3) = sum over j (B-neighbour order) of sum_n2 c(n1,n2) * b(n3,n2)
+// With `exact` the multiply and the add of every term round separately, which
+// reproduces the default kernel built without FMA contraction bit for bit.
+// No atomics, no reduction trees: results are deterministic and independent of
+// the launch shape.
+//
+// The bound is the L2/HBM traffic of the operand blocks (an nd x nd FP64 block
+// pair per triple, 2 nd^3 flops): for nd = 4 this is 256 B per 128 flops.
+#include "cq_internal.hpp"
+
+namespace cqb {
+namespace {
+
+template <bool EXACT>
+__device__ __forceinline__ double madd(double acc, double x, double y) {
+  if (EXACT) return __dadd_rn(acc, __dmul_rn(x, y));
+  return fma(x, y, acc);
+}
+
+struct MultArgs {
+  const int64_t* __restrict__ ptr;   // [n_out+1]
+  const int2* __restrict__ pairs;    // (x block, b block)
+  int n_out;
+  // output blocks
+  const int* __restrict__ o_row;
+  const int* __restrict__ o_cover;
+  const int64_t* __restrict__ o_elem;
+  // first operand blocks (type 1: A; type 2: the input c)
+  const int* __restrict__ x_cover;
+  const int64_t* __restrict__ x_elem;
+  // B blocks
+  const int64_t* __restrict__ b_elem;
+  const int* __restrict__ b_cover;
+  const int* __restrict__ prim_nsf;
+  const int* __restrict__ cover_nsf;
+  const double* __restrict__ x;
+  const double* __restrict__ b;
+  double* __restrict__ out;
+};
+
+// Generic block sizes (nd <= 16): one warp per output block, up to 8 elements per lane.
+template <int TYPE, bool EXACT>
+__global__ void __launch_bounds__(256) k_mult_generic(MultArgs M) {
+  int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (q >= M.n_out) return;
+  const int ndi = M.prim_nsf[M.o_row[q]];
+  const int ndo = M.cover_nsf[M.o_cover[q]];    // type 1: nd_j ; type 2: nd_k
+  const int ne = ndi * ndo;
+  double acc[8];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) acc[r] = 0.0;
+  const int64_t p0 = M.ptr[q], p1 = M.ptr[q + 1];
+  for (int64_t t = p0; t < p1; ++t) {
+    int2 pr = M.pairs[t];
+    const double* X = M.x + M.x_elem[pr.x];
+    const double* B = M.b + M.b_elem[pr.y];
+    if (TYPE == 1) {
+      const int ndk = M.cover_nsf[M.x_cover[pr.x]];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        int e = lane + 32 * r;
+        if (e < ne) {
+          int n1 = e % ndi, n2 = e / ndi;
+          double a = acc[r];
+          for (int n3 = 0; n3 < ndk; ++n3) a = madd<EXACT>(a, X[n1 + ndi * n3], B[n3 + ndk * n2]);
+          acc[r] = a;
+        }
+      }
+    } else {
+      const int ndj = M.cover_nsf[M.b_cover[pr.y]];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        int e = lane + 32 * r;
+        if (e < ne) {
+          int n1 = e % ndi, n3 = e / ndi;
+          double a = acc[r];
+          for (int n2 = 0; n2 < ndj; ++n2) a = madd<EXACT>(a, X[n1 + ndi * n2], B[n3 + ndo * n2]);
+          acc[r] = a;
+        }
+      }
+    }
+  }
+  double* O = M.out + M.o_elem[q];
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    int e = lane + 32 * r;
+    if (e < ne) O[e] = acc[r];
+  }
+}
+
+// 4 x 4 blocks (SZ basis): 16 lanes per output block, one element per lane.  Each lane
+// loads its operand row/column as two 16-byte vectors per block; blocks are 128 B aligned.
+template <int TYPE, bool EXACT>
+__global__ void __launch_bounds__(256) k_mult_nd4(MultArgs M) {
+  int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 4, l = threadIdx.x & 15;
+  if (g >= M.n_out) return;
+  const int n1 = l & 3, m = l >> 2;   // element (n1, m) of the output block
+  double acc = 0.0;
+  const int64_t p0 = M.ptr[g], p1 = M.ptr[g + 1];
+  for (int64_t t = p0; t < p1; ++t) {
+    int2 pr = M.pairs[t];
+    const double* X = M.x + M.x_elem[pr.x];
+    const double* B = M.b + M.b_elem[pr.y];
+    if (TYPE == 1) {
+      // c(n1,m) += sum_n3 a(n1,n3) b(n3,m): a row is strided, b column contiguous
+      double2 b01 = __ldg(reinterpret_cast<const double2*>(B + 4 * m));
+      double2 b23 = __ldg(reinterpret_cast<const double2*>(B + 4 * m + 2));
+      acc = madd<EXACT>(acc, __ldg(X + n1), b01.x);
+      acc = madd<EXACT>(acc, __ldg(X + n1 + 4), b01.y);
+      acc = madd<EXACT>(acc, __ldg(X + n1 + 8), b23.x);
+      acc = madd<EXACT>(acc, __ldg(X + n1 + 12), b23.y);
+    } else {
+      // a(n1,m) += sum_n2 c(n1,n2) b(m,n2)
+      acc = madd<EXACT>(acc, __ldg(X + n1), __ldg(B + m));
+      acc = madd<EXACT>(acc, __ldg(X + n1 + 4), __ldg(B + m + 4));
+      acc = madd<EXACT>(acc, __ldg(X + n1 + 8), __ldg(B + m + 8));
+      acc = madd<EXACT>(acc, __ldg(X + n1 + 12), __ldg(B + m + 12));
+    }
+  }
+  M.out[M.o_elem[g] + l] = acc;
+}
+
+// One drop-in m_kern_max (type 1) / m_kern_min (type 2) call: output blocks with explicit
+// offsets, accumulated in place in the layouts mat_mult passes (type 1 reads the local
+// transpose a(n3 + nd3*n1); type 2 accumulates into it).  One warp per output block.
+__global__ void __launch_bounds__(256) k_dropin(int type, const int64_t* __restrict__ out_off, const int* __restrict__ dims,
+                                                const int64_t* __restrict__ ptr, const int64_t* __restrict__ pairs, int n_out,
+                                                const double* __restrict__ x, const double* __restrict__ b,
+                                                double* __restrict__ out) {
+  int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (q >= n_out) return;
+  const int r = dims[2 * q], cols = dims[2 * q + 1], ne = r * cols;
+  double* O = out + out_off[q];
+  for (int e = lane; e < ne; e += 32) {
+    double acc = O[e];
+    if (type == 1) {
+      int n1 = e % r, n2 = e / r;
+      for (int64_t t = ptr[q]; t < ptr[q + 1]; ++t) {
+        const double* X = x + pairs[3 * t];
+        const double* B = b + pairs[3 * t + 1];
+        int nd3 = (int)pairs[3 * t + 2];
+        for (int n3 = 0; n3 < nd3; ++n3) acc = madd<true>(acc, X[n3 + nd3 * n1], B[n3 + nd3 * n2]);
+      }
+    } else {
+      int n3 = e % cols, n1 = e / cols;   // atrans block: nd3 x nd1, n3 fastest
+      for (int64_t t = ptr[q]; t < ptr[q + 1]; ++t) {
+        const double* X = x + pairs[3 * t];
+        const double* B = b + pairs[3 * t + 1];
+        int nd2 = (int)pairs[3 * t + 2];
+        for (int n2 = 0; n2 < nd2; ++n2) acc = madd<true>(acc, X[n1 + r * n2], B[n3 + cols * n2]);
+      }
+    }
+    O[e] = acc;
+  }
+}
+
+}  // namespace
+
+void launch_dropin(int type, const int64_t* d_out, const int* d_dims, const int64_t* d_ptr, const int64_t* d_pairs,
+                   int n_out, const double* x, const double* b, double* out, cudaStream_t st) {
+  if (n_out <= 0) return;
+  int grid = (int)(((int64_t)n_out * 32 + 255) / 256);
+  k_dropin<<<grid, 256, 0, st>>>(type, d_out, d_dims, d_ptr, d_pairs, n_out, x, b, out);
+  CQ_CUDA(cudaGetLastError());
+}
+
+void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, double* c, int exact) {
+  RangeIndex &A = *S.ranges[P.ra], &B = *S.ranges[P.rb], &C = *S.ranges[P.rc];
+  MultArgs M;
+  M.ptr = P.ptr.p;
+  M.pairs = P.pairs.p;
+  M.b_elem = B.nb_elem.p;
+  M.b_cover = B.nb_cover.p;
+  M.prim_nsf = S.dg.prim_nsf.p;
+  M.cover_nsf = S.dg.cover_nsf.p;
+  M.b = b;
+  RangeIndex& O = P.mult_type == 1 ? C : A;
+  RangeIndex& X = P.mult_type == 1 ? A : C;
+  M.n_out = O.nnz;
+  M.o_row = O.nb_row.p; M.o_cover = O.nb_cover.p; M.o_elem = O.nb_elem.p;
+  M.x_cover = X.nb_cover.p; M.x_elem = X.nb_elem.p;
+  M.x = P.mult_type == 1 ? a : c;
+  M.out = P.mult_type == 1 ? c : a;
+  if (M.n_out == 0) return;
+  cudaStream_t st = S.stream;
+  const int T = 256;
+  // the 4 x 4 path reads B with 16-byte vector loads: require 16-byte aligned operands
+  bool aligned = ((uintptr_t)b % 16 == 0) && ((uintptr_t)M.x % 16 == 0);
+  if (S.uniform_nsf == 4 && aligned) {
+    int grid = (int)(((int64_t)M.n_out * 16 + T - 1) / T);
+    if (P.mult_type == 1) {
+      if (exact) k_mult_nd4<1, true><<<grid, T, 0, st>>>(M); else k_mult_nd4<1, false><<<grid, T, 0, st>>>(M);
+    } else {
+      if (exact) k_mult_nd4<2, true><<<grid, T, 0, st>>>(M); else k_mult_nd4<2, false><<<grid, T, 0, st>>>(M);
+    }
+  } else {
+    int grid = (int)(((int64_t)M.n_out * 32 + T - 1) / T);
+    if (P.mult_type == 1) {
+      if (exact) k_mult_generic<1, true><<<grid, T, 0, st>>>(M); else k_mult_generic<1, false><<<grid, T, 0, st>>>(M);
+    } else {
+      if (exact) k_mult_generic<2, true><<<grid, T, 0, st>>>(M); else k_mult_generic<2, false><<<grid, T, 0, st>>>(M);
+    }
+  }
+  CQ_CUDA(cudaGetLastError());
+}
+
+}  // namespace cqb

@@ -1,0 +1,210 @@
+/*
+ * cq_b200.h -- C ABI of the B200-native CONQUEST block-sparse multiply and
+ * LNV / McWeeny density-matrix solver (libcqb200.so).
+ *
+ * Conventions shared with the reference (OrderN/CONQUEST-release):
+ *   - A block-sparse matrix of range r is one flat FP64 array holding, for each
+ *     primary atom i (partition order) and each neighbour j within r (covering
+ *     set order, periodic images distinct), an nd_i x nd_j block stored column
+ *     major (i orbital fastest).  This is the storage of `mat_p(A)%matrix`
+ *     (src/mult_module.f90) built by get_naba / make_halo
+ *     (src/matrix_elements_module.f90:257-716).
+ *   - mult_type 1 computes C = A.B (C overwritten); mult_type 2 computes
+ *     a = c.b^T restricted to the range of a (a overwritten), with the argument
+ *     roles of mat_mult (src/multiply_module.f90:115).
+ *   - Every entry point returns 0 on success or a CQ_ERR_* code; the message of
+ *     the last failure is returned by cq_last_error().  The Fortran shim maps a
+ *     nonzero status to cq_abort (src/GenComms/generic_comms.f90:95).
+ *
+ * Pointers named *_dev are device (HBM) pointers; every other pointer is host
+ * memory.  Calls on one system are stream ordered and not re-entrant.
+ */
+#ifndef CQ_B200_H
+#define CQ_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CQ_OK 0
+#define CQ_ERR_ARG 1          /* invalid argument or unknown range / product */
+#define CQ_ERR_OOM 2          /* device allocation failed */
+#define CQ_ERR_CUDA 3         /* CUDA runtime error */
+#define CQ_ERR_BOUNDS 4       /* an index check failed (the kernel skipped the access) */
+#define CQ_ERR_TIMEOUT 5      /* a bounded wait ran out */
+#define CQ_ERR_STATE 6        /* call not valid in the current state */
+#define CQ_ERR_NOT_CONVERGED 7
+
+typedef struct cq_system cq_system;
+
+/* Last error message of the calling thread (static storage, never NULL). */
+const char* cq_last_error(void);
+
+/* Library version string. */
+const char* cq_version(void);
+
+/*
+ * Geometry and index construction for one periodic system on one GPU.
+ * Replaces the one-process path of sfc_partitions_to_processors
+ * (src/sfc_partitions_module.f90:124), make_prim (src/primary_module.f90:97),
+ * make_cs (src/cover_module.f90:133) and matrix_ini for every listed range
+ * (src/matrix_elements_module.f90:67-142, called from immi,
+ * src/mult_module.f90:271).  The covering set is built for the largest range.
+ *   coords[3*n]  Cartesian positions (bohr), wrapped into the cell as
+ *                read_atomic_positions does (src/io_module.f90:418)
+ *   cell[3]      orthorhombic cell lengths
+ *   nsf[n]       block size (support functions) of each atom
+ *   rcuts[n_ranges] matrix ranges; range r is addressed by its position
+ *   max_atoms_part General.MaxAtomsPartition (reference default 34)
+ *   gap_threshold, avg_atomic_diameter  General.GapThreshold / AverageAtomicDiameter
+ * The neighbour lists, halos, retro lists and transposes are built on the GPU.
+ */
+int cq_system_create(int n_atoms, const double* coords, const double* cell, const int* nsf, int n_ranges,
+                     const double* rcuts, int max_atoms_part, double gap_threshold, double avg_atomic_diameter,
+                     cq_system** out);
+int cq_system_destroy(cq_system* sys);
+
+/* Number of stored elements (mat_p(A)%length) and blocks of range r. */
+int cq_range_length(cq_system* sys, int r, int64_t* length, int64_t* n_blocks);
+
+/*
+ * Export one index array of range r (r < 0: a geometry array) as int64, in the
+ * reference's 1-based conventions, for bit-exact parity checks.  Names:
+ *   geometry: "n_parts", "cover_dims", "ngnode", "nm_group", "ig_prim",
+ *             "lab_cell", "lab_cover", "n_ing_cover", "icover_ibeg", "ig_cover", "iprim_group"
+ *   range:    "n_nab", "i_acc", "i_nd_acc", "ndimi", "onsite", "i_part", "i_seq",
+ *             "ndimj", "npxyz", "bind", "halo_sizes", "nh_part", "j_beg",
+ *             "lab_hcell", "lab_hcover", "j_seq", "halo_ndimj", "i_halo", "i_h2d",
+ *             "t_i_prim", "t_i_beg", "t_i_nd_beg", "t_n_hnab", "itran_addr"
+ * With out == NULL only *n is set.
+ */
+int cq_export_index(cq_system* sys, int r, const char* name, int64_t* out, int64_t cap, int64_t* n);
+
+/* Radii of the stored blocks of range r (matrix%radius), nnz entries. */
+int cq_export_radius(cq_system* sys, int r, double* out, int64_t cap, int64_t* n);
+
+/*
+ * mat_mult on device-resident operands (src/multiply_module.f90:115-359 with
+ * the m_kern_max / m_kern_min summation order of
+ * src/multiply_kernel_default.f90:132-224, 325-412).
+ *   mult_type 1: c_dev (range rc) = a_dev (range ra) . b_dev (range rb)
+ *   mult_type 2: a_dev (range ra) = c_dev (range rc) . b_dev^T (range rb)
+ * exact != 0 keeps the reference's separate multiply and add per term
+ * (bit-identical to the default kernel built without FMA contraction);
+ * exact == 0 fuses them.  The pair lists of the product are built on the
+ * first call and cached.  Work is enqueued on the system's stream; the call
+ * returns without synchronising.
+ */
+int cq_mat_mult(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a_dev, const double* b_dev,
+                double* c_dev, int exact);
+
+/* Same as cq_mat_mult with host arrays: copies in, multiplies, copies the result out, synchronises. */
+int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c,
+                     int exact);
+
+/* Algorithmic work of one product: (k,i,j) triples with a stored result and 2*sum nd^3 flops. */
+int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* triples, int64_t* flops);
+
+/*
+ * Drop-in kernel pair (plugin surface of multiply_kernel_<MULT_KERN>.f90):
+ * the argument lists of m_kern_max / m_kern_min
+ * (src/multiply_kernel_default.f90:132-160, 325-358) with the derived types
+ * flattened into their component arrays (Fortran 1-based values, host memory):
+ *   ahalo: nh_part, j_beg, j_seq, ndimi, ndimj
+ *   chalo: i_halo, i_hbeg, i_h2d (n_prim*ni_in_halo), ni_in_halo
+ *   at   : i_prim, i_beg, i_nd_beg, n_hnab
+ * a(lena) is the local transpose (type 1) or the accumulator (type 2),
+ * b(lenb) the partition's B data, c(lenc) the accumulator (type 1) or input
+ * (type 2); the accumulator is updated in place on return, exactly as one call
+ * of the default kernel for partition kpart.
+ */
+int cq_m_kern_max(int k_off, int kpart, const int* ib_nd_acc, const int* ibaddr, const int* nbnab, const int* ibpart,
+                  const int* ibseq, const int* bndim2, const double* a, const double* b, double* c,
+                  const int* ahalo_nh_part, const int* ahalo_j_beg, const int* ahalo_j_seq, const int* ahalo_ndimi,
+                  const int* ahalo_ndimj, const int* chalo_i_halo, const int* chalo_i_hbeg, const int* chalo_i_h2d,
+                  int chalo_ni_in_halo, const int* at_i_prim, const int* at_i_beg, const int* at_i_nd_beg,
+                  const int* at_n_hnab, int mx_absb, int mx_part, int mx_iprim, int lena, int lenb, int lenc);
+int cq_m_kern_min(int k_off, int kpart, const int* ib_nd_acc, const int* ibaddr, const int* nbnab, const int* ibpart,
+                  const int* ibseq, const int* bndim2, double* a, const double* b, const double* c,
+                  const int* ahalo_nh_part, const int* ahalo_j_beg, const int* ahalo_j_seq, const int* ahalo_ndimi,
+                  const int* ahalo_ndimj, const int* chalo_i_halo, const int* chalo_i_hbeg, const int* chalo_i_h2d,
+                  int chalo_ni_in_halo, const int* at_i_prim, const int* at_i_beg, const int* at_i_nd_beg,
+                  const int* at_n_hnab, int mx_absb, int mx_part, int mx_iprim, int lena, int lenb, int lenc);
+
+/* matrix_sum (src/mult_module.f90:2677-2715): a = alpha*a + beta*b; ranges may differ (matrix_add rules). */
+int cq_matrix_sum(cq_system* sys, int ra, double* a_dev, double alpha, int rb, const double* b_dev, double beta);
+/* matrix_transpose within one range (src/mult_module.f90:2609-2673). */
+int cq_matrix_transpose(cq_system* sys, int r, const double* a_dev, double* at_dev);
+/* matrix_trace (src/mult_module.f90:2773-2811) and matrix_product_trace (2885-2916). */
+int cq_matrix_trace(cq_system* sys, int r, const double* a_dev, double* result);
+int cq_matrix_product_trace(cq_system* sys, int r, const double* a_dev, const double* b_dev, double* result);
+
+/* Synchronise the system's stream. */
+int cq_synchronize(cq_system* sys);
+
+/* ------------------------------------------------------------------------ */
+/* LNV / McWeeny density-matrix minimisation (one spin channel, nspin = 1)   */
+/* ------------------------------------------------------------------------ */
+typedef struct cq_lnv cq_lnv;
+
+/* Control parameters; defaults are the reference's fdf defaults
+ * (src/initial_read_module.f90:1208, 1598-1608, 1901-1904). */
+typedef struct {
+  int n_L_iterations;      /* DM.LVariations (50) */
+  double tolerance;        /* minE.LTolerance (1e-7) */
+  int maxpulay;            /* DM.MaxPulay (5) */
+  double minpulaystep;     /* DM.MinPulayStepSize (1e-3) */
+  double maxpulaystep;     /* DM.MaxPulayStepSize (0.1) */
+  double lintol;           /* DM.LinTol (0.1) */
+  int global_tolerance;    /* minE.GlobalTolerance (0 for static runs) */
+  int vary_mu;             /* !DM.ConstantMu (1) */
+  int invs_max_steps;      /* DM.InvSMaxSteps (100) */
+  double invs_delta_tol;   /* DM.InvSDeltaOmegaTolerance (1e-4) */
+  double invs_tol;         /* DM.InvSTolerance (1e-2) */
+  int exact;               /* 1: FP64 products with the default kernel's rounding; 0: fused multiply-add */
+  int max_outer;           /* bound on FindMinDM outer iterations (the reference loops until done) */
+} cq_lnv_params;
+
+typedef struct {
+  double energy;           /* band energy 2 Tr(K H), K = 3LSL - 2LSLSL */
+  double electrons;        /* 2 (3 Tr(L SLS) - 2 Tr(L SLSLS)) */
+  double residual;         /* last DM residual g (per atom unless global_tolerance) */
+  double invs_omega;       /* Hotelling residual of T = S^-1 */
+  int mcw_sweeps, early_iters, late_iters, ne_corrections, inflexions, converged;
+  int64_t n_products;      /* block-sparse products executed */
+  int64_t flops;           /* algorithmic flops of those products (2 sum nd_i nd_j nd_k) */
+} cq_lnv_result;
+
+int cq_lnv_params_default(cq_lnv_params* p);
+
+/*
+ * Density-matrix solver on a system.  ranges[11] gives the system range index
+ * of S, H, L, T, LS, LH, LSL, SLS, TS, TH, TL in that order (rcut(LS) = L + S,
+ * rcut(LSL) = 2L + S ... as src/dimens_module.f90:338-355; SL, HL, LTr, TTr
+ * share the index of LS, LH, L, T).  ne_spin = ne_spin_in_cell(1).
+ */
+int cq_lnv_create(cq_system* sys, const int* ranges, double ne_spin, const cq_lnv_params* p, cq_lnv** out);
+int cq_lnv_destroy(cq_lnv* s);
+/* Load S and H (range layouts of S and H) from host or device memory. */
+int cq_lnv_set_SH(cq_lnv* s, const double* S, const double* H, int on_device);
+/* T = S^-1 by Hotelling iterations (Iter_Hott_InvS, src/S_matrix_module.f90:746-963); omega returned. */
+int cq_lnv_invert_S(cq_lnv* s, double* omega);
+/* FindMinDM (src/DMMinModule.f90:172-312); resetL != 0 starts from the McWeeny initial L. */
+int cq_lnv_find_min_dm(cq_lnv* s, int resetL, cq_lnv_result* res);
+/* Copy one matrix out: name in "L", "K", "T", "S", "H", "phi"; to host (on_device = 0) or device memory. */
+int cq_lnv_get(cq_lnv* s, const char* name, double* out, int64_t cap, int on_device);
+/* Copy a matrix in (for example a previous L): name in "L", "T". */
+int cq_lnv_put(cq_lnv* s, const char* name, const double* in, int on_device);
+/*
+ * One complete solve from host arrays: load S and H, T = S^-1, FindMinDM from
+ * the McWeeny start, copy L and K back (either may be NULL).  This is the
+ * end-to-end call of a user holding S and H in host memory.
+ */
+int cq_lnv_solve_host(cq_lnv* s, const double* S, const double* H, double* L_out, double* K_out, cq_lnv_result* res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CQ_B200_H */

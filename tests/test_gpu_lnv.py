@@ -1,0 +1,69 @@
+"""GPU LNV / McWeeny chain vs the oracle chain and vs the exact dense answer.
+
+Tolerances (north star): band energy and electron count within 1e-10 of the
+oracle for the FP64 path.
+"""
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+import blockmaps as bm
+import systems
+from cq_b200 import inputs
+from cq_oracle import OracleSystem
+from lnv_oracle import OracleLNV, Params
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(coords, cell, nsf, ne_spin, rs=10.0, rh=12.0, rl=16.0, rt=10.0, **params):
+    import cq_b200
+    rng = cq_b200.lnv_ranges(rs, rh, rl, rt)
+    names = list(rng)
+    ridx = {n: i for i, n in enumerate(names)}
+    o = OracleSystem(coords, cell, nsf, list(rng.values()))
+    g = cq_b200.System(coords, cell, nsf, list(rng.values()))
+    blS = bm.oracle_blocklist(o, ridx["S"], coords, cell)
+    blH = bm.oracle_blocklist(o, ridx["H"], coords, cell)
+    S, H = inputs.overlap_S(blS), inputs.hamiltonian_H(blH, seed=5)
+    olnv = OracleLNV(o, ridx, S, H, ne_spin, float(np.sum(nsf)), Params(**params))
+    glnv = cq_b200.LNV(g, ridx, ne_spin, **params)
+    return o, g, ridx, S, H, olnv, glnv
+
+
+def _dense(bl, v, n, nd):
+    M = np.zeros((n * nd, n * nd))
+    for q in range(len(bl.ig_i)):
+        i, j = bl.ig_i[q], bl.ig_j[q]
+        M[i * nd:(i + 1) * nd, j * nd:(j + 1) * nd] += v[bl.elem_off[q]:bl.elem_off[q] + nd * nd].reshape(nd, nd).T
+    return M
+
+
+def test_cluster_matches_dense_eigh():
+    """No truncation (ranges exceed the cluster): the LNV minimum is the exact ground state."""
+    coords, cell = inputs.si_cluster(64, sigma=0.1, seed=4)
+    n = len(coords)
+    diam = np.max(np.linalg.norm(coords[:, None] - coords[None], axis=-1))
+    ne_spin = 64.0
+    o, g, ridx, S, H, olnv, glnv = _setup(coords, cell, np.full(n, 4), ne_spin, rl=diam + 1, rt=diam + 1)
+    res, L, K = glnv.solve_host(S, H, want_L=True, want_K=True)
+    blS = bm.oracle_blocklist(o, ridx["S"], coords, cell); blH = bm.oracle_blocklist(o, ridx["H"], coords, cell)
+    ev = sla.eigh(_dense(blH, H, n, 4), _dense(blS, S, n, 4), eigvals_only=True)
+    exact = 2.0 * ev[:int(ne_spin)].sum()
+    assert res["converged"] == 1
+    assert abs(res["energy"] - exact) < 1e-9 * abs(exact)
+    assert abs(res["electrons"] - 2 * ne_spin) < 1e-8
+
+
+def test_config2_small_matches_oracle_chain():
+    """Periodic Si (2x2x2 cells, SZ, truncated ranges): GPU chain vs oracle chain within 1e-10."""
+    coords, cell = inputs.diamond_si(2, sigma=0.1, seed=2)
+    n = len(coords)
+    ne_spin = float(n)   # 2 electrons per atom
+    o, g, ridx, S, H, olnv, glnv = _setup(coords, cell, np.full(n, 4), ne_spin)
+    olnv.iter_hott_invs()
+    E_o, N_o = olnv.find_min_dm()
+    res, L, K = glnv.solve_host(S, H, want_L=True)
+    assert res["converged"] == 1
+    assert abs(res["energy"] - E_o) <= 1e-10 * max(1.0, abs(E_o))
+    assert abs(res["electrons"] - N_o) <= 1e-10 * max(1.0, abs(N_o))

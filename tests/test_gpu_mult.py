@@ -1,0 +1,154 @@
+"""GPU mat_mult, drop-in kernels and algebra vs the oracle.
+
+FP64 with exact=True keeps the default kernel's separate multiply and add per
+term in the same order, so results must equal the oracle bit for bit.  The
+fused variant (exact=False) must stay within 1e-12 relative per element,
+measured against sum |a||b| of the element's terms.
+"""
+import numpy as np
+import pytest
+
+import blockmaps as bm
+import dropin_driver
+import systems
+from cq_b200 import inputs
+from cq_oracle import OracleSystem
+
+pytestmark = pytest.mark.gpu
+
+
+def _sys(coords, cell, nsf, rc):
+    import cq_b200
+    return OracleSystem(coords, cell, nsf, rc), cq_b200.System(coords, cell, nsf, rc)
+
+
+@pytest.fixture(scope="module")
+def cfg1():
+    coords, cell, nsf, rc = systems.config1()
+    o, g = _sys(coords, cell, nsf, rc)
+    bls = [bm.oracle_blocklist(o, r, coords, cell) for r in range(len(rc))]
+    return o, g, bls
+
+
+@pytest.fixture(scope="module")
+def cfg2():
+    coords, cell, nsf = systems.config2()
+    rng = systems.lnv_ranges()
+    names = list(rng.keys())
+    o, g = _sys(coords, cell, nsf, list(rng.values()))
+    bls = {n: bm.oracle_blocklist(o, i, coords, cell) for i, n in enumerate(names)}
+    idx = {n: i for i, n in enumerate(names)}
+    return o, g, bls, idx
+
+
+def _abs_bound(o, mult_type, ra, rb, rc, a, b, c):
+    """sum |a||b| per output element, from the oracle run on absolute values."""
+    aa, bb, cc = np.abs(a), np.abs(b), np.abs(c)
+    if mult_type == 1:
+        out = np.zeros_like(c)
+        o.mat_mult(1, ra, rb, rc, aa, bb, out)
+    else:
+        out = np.zeros_like(a)
+        o.mat_mult(2, ra, rb, rc, out, bb, cc)
+    return out
+
+
+def test_type1_dzp_bit_exact(cfg1):
+    o, g, bls = cfg1
+    a = inputs.random_blocks(bls[0], 11, inputs.TAG_RANDOM_A)
+    b = inputs.random_blocks(bls[1], 11, inputs.TAG_RANDOM_B)
+    c_ref = np.zeros(bls[2].length)
+    o.mat_mult(1, 0, 1, 2, a, b, c_ref)
+    c = np.full(bls[2].length, np.nan)
+    g.mat_mult_host(1, 0, 1, 2, a, b, c, exact=True)
+    assert np.array_equal(c, c_ref)
+    c2 = np.zeros(bls[2].length)
+    g.mat_mult_host(1, 0, 1, 2, a, b, c2, exact=False)
+    bound = _abs_bound(o, 1, 0, 1, 2, a, b, c_ref)
+    assert np.all(np.abs(c2 - c_ref) <= 1e-12 * bound + 1e-300)
+    # algorithmic work matches the triple count of the default kernel
+    t, f = g.product_work(1, 0, 1, 2)
+    assert f == 2 * 13 ** 3 * t and t > 0
+
+
+def test_type2_dzp_bit_exact(cfg1):
+    o, g, bls = cfg1
+    b = inputs.random_blocks(bls[1], 12, inputs.TAG_RANDOM_B)
+    cin = inputs.random_blocks(bls[2], 12, inputs.TAG_RANDOM_A)
+    out_ref = np.zeros(bls[0].length)
+    o.mat_mult(2, 0, 1, 2, out_ref, b, cin)
+    out = np.full(bls[0].length, np.nan)
+    g.mat_mult_host(2, 0, 1, 2, out, b, cin, exact=True)
+    assert np.array_equal(out, out_ref)
+
+
+LNV_PRODUCTS = [  # (type, a range, b range, c range) in mat_mult roles, from the product table of mult_module.f90
+    (1, "L", "S", "LS"), (1, "L", "H", "LH"), (1, "LH", "S", "LSL"), (2, "L", "LS", "LSL"), (1, "LS", "S", "SLS"),
+    (2, "L", "LS", "SLS"), (1, "LS", "L", "LSL"), (2, "H", "LS", "LSL"), (1, "T", "L", "TL"), (2, "L", "T", "TL"),
+    (1, "T", "S", "TS"), (1, "T", "H", "TH"), (2, "L", "T", "TH"), (2, "T", "T", "TS"),
+]
+
+
+@pytest.mark.parametrize("prod", LNV_PRODUCTS)
+def test_lnv_products_sz_bit_exact(cfg2, prod):
+    o, g, bls, idx = cfg2
+    t, ra, rb, rc = prod
+    ia, ib, ic = idx[ra], idx[rb], idx[rc]
+    a = inputs.random_blocks(bls[ra], 21, inputs.TAG_RANDOM_A)
+    b = inputs.random_blocks(bls[rb], 21, inputs.TAG_RANDOM_B)
+    c = inputs.random_blocks(bls[rc], 22, inputs.TAG_RANDOM_A)
+    if t == 1:
+        ref = np.zeros(bls[rc].length); o.mat_mult(1, ia, ib, ic, a, b, ref)
+        got = np.full(bls[rc].length, np.nan); g.mat_mult_host(1, ia, ib, ic, a, b, got)
+    else:
+        ref = np.zeros(bls[ra].length); o.mat_mult(2, ia, ib, ic, ref, b, c)
+        got = np.full(bls[ra].length, np.nan); g.mat_mult_host(2, ia, ib, ic, got, b, c)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("mult_type", [1, 2])
+def test_dropin_kernels_match_default(cfg2, mult_type):
+    """mat_mult's partition loop calling cq_m_kern_max / cq_m_kern_min reproduces the default kernel."""
+    o, g, bls, idx = cfg2
+    ra, rb, rc = ("L", "S", "LS") if mult_type == 1 else ("L", "LS", "SLS")
+    ia, ib, ic = idx[ra], idx[rb], idx[rc]
+    a = inputs.random_blocks(bls[ra], 31, inputs.TAG_RANDOM_A)
+    b = inputs.random_blocks(bls[rb], 31, inputs.TAG_RANDOM_B)
+    c = inputs.random_blocks(bls[rc], 32, inputs.TAG_RANDOM_A)
+    if mult_type == 1:
+        ref = np.zeros(bls[rc].length); o.mat_mult(1, ia, ib, ic, a, b, ref)
+        got = np.zeros(bls[rc].length); dropin_driver.mat_mult_dropin(o, 1, ia, ib, ic, a, b, got)
+    else:
+        ref = np.zeros(bls[ra].length); o.mat_mult(2, ia, ib, ic, ref, b, c)
+        got = np.zeros(bls[ra].length); dropin_driver.mat_mult_dropin(o, 2, ia, ib, ic, got, b, c)
+    assert np.array_equal(got, ref)
+
+
+def test_algebra_matches_oracle(cfg2):
+    import torch
+    o, g, bls, idx = cfg2
+    dev = torch.device("cuda:0")
+    L = inputs.random_blocks(bls["L"], 41, 1)
+    S = inputs.random_blocks(bls["S"], 41, 2)
+    LSL = inputs.random_blocks(bls["LSL"], 41, 3)
+    tL, tS, tLSL = (torch.tensor(x, device=dev) for x in (L, S, LSL))
+    # same range: scal + axpy
+    ref = L.copy(); ref = ref * 0.5; ref = ref + (-2.0 * L)
+    t = tL.clone(); g.matrix_sum(idx["L"], t, 0.5, idx["L"], tL, -2.0); g.synchronize()
+    assert np.array_equal(t.cpu().numpy(), ref)
+    # shorter destination (prune) and longer destination (partial update)
+    ref = S.copy(); o.matrix_add(0.0, ref, idx["S"], 3.0, LSL, idx["LSL"])
+    t = tS.clone(); g.matrix_sum(idx["S"], t, 0.0, idx["LSL"], tLSL, 3.0); g.synchronize()
+    assert np.array_equal(t.cpu().numpy(), ref)
+    ref = L.copy(); o.matrix_add(1.0, ref, idx["L"], -0.25, S, idx["S"])
+    t = tL.clone(); g.matrix_sum(idx["L"], t, 1.0, idx["S"], tS, -0.25); g.synchronize()
+    assert np.array_equal(t.cpu().numpy(), ref)
+    # transpose, traces
+    for r in ("L", "LS", "LSL"):
+        x = inputs.random_blocks(bls[r], 43, 5)
+        tx = torch.tensor(x, device=dev); tt = torch.empty_like(tx)
+        g.transpose(idx[r], tx, tt); g.synchronize()
+        assert np.array_equal(tt.cpu().numpy(), o.transpose(idx[r], x))
+    assert abs(g.trace(idx["L"], tL) - o.trace(idx["L"], L)) < 1e-12 * abs(o.trace(idx["L"], L)) + 1e-14
+    dot_ref = float(np.dot(L, L))
+    assert abs(g.product_trace(idx["L"], tL, tL) - dot_ref) < 1e-12 * dot_ref
