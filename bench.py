@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 LNV / McWeeny density-matrix solver (libcqb200.so).
+
+Workload (N=1 default): plain FP64 LNV + McWeeny density-matrix minimisation on a
+512-atom diamond Si supercell (4x4x4 conventional cells, a = 10.263 bohr, seeded
+displacements sigma = 0.1 bohr), 4x4 (SZ) blocks, S range 10, H range 12,
+L range 16, T range 10 bohr, 1024 electrons, DM.LVariations = 50, tolerance 1e-7.
+One step = one complete solve on device-resident S and H: T = S^-1 by Hotelling
+iterations, then FindMinDM from the McWeeny initial L.  Synthetic seeded inputs.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun, one rank per GPU): independent replicas, one solve per rank
+per step, no collectives on the data path (weak scaling); time is the max over
+ranks.  `--impl reference` times the CPU restatement of the reference's
+multiply_kernel_ompGemm chain on the host cores instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "conquest-release_b200"))
+
+METRIC = "LNV solves/s (FP64, 512-atom Si SZ)"
+WORKLOAD = "lnv512_si_sz_fp64"
+CFG = dict(ncell=4, sigma=0.1, seed=2, rs=10.0, rh=12.0, rl=16.0, rt=10.0, nsf=4, ne_per_atom=2.0, h_seed=5)
+
+
+def build_problem(cq_b200):
+    """System, solver and host S/H of the workload (setup, untimed)."""
+    from cq_b200 import inputs
+    coords, cell = inputs.diamond_si(CFG["ncell"], sigma=CFG["sigma"], seed=CFG["seed"])
+    n = len(coords)
+    rng = cq_b200.lnv_ranges(CFG["rs"], CFG["rh"], CFG["rl"], CFG["rt"])
+    names = list(rng)
+    ridx = {k: i for i, k in enumerate(names)}
+    sysm = cq_b200.System(coords, cell, np.full(n, CFG["nsf"], np.int32), list(rng.values()))
+    blS = sysm.blocklist(ridx["S"], coords, cell)
+    blH = sysm.blocklist(ridx["H"], coords, cell)
+    S = inputs.overlap_S(blS)
+    H = inputs.hamiltonian_H(blH, seed=CFG["h_seed"])
+    ne_spin = CFG["ne_per_atom"] * n / 2.0
+    solver = cq_b200.LNV(sysm, ridx, ne_spin, exact=1)
+    return dict(coords=coords, cell=cell, n=n, ridx=ridx, system=sysm, S=S, H=H, solver=solver, ne_spin=ne_spin)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary (None if absent)."""
+    p = os.path.join(ROOT, "profiles", "lnv512_mult_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p)).get("dram_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+def work_record_path():
+    return os.path.join(ROOT, "profiles", "lnv512_solve_work.json")
+
+
+def lnv_call_products():
+    """The products of one LNV_matrix_multiply(doM3, dophi, doE) call (mult_module.f90:1557-1700), mat_mult roles."""
+    return [(1, "L", "S", "LS"), (1, "L", "H", "LH"), (1, "LH", "S", "LSL"), (1, "LH", "S", "LSL"),
+            (2, "L", "LS", "LSL"), (1, "LS", "S", "SLS"), (2, "L", "LS", "SLS"), (1, "LS", "L", "LSL"),
+            (2, "H", "LS", "LSL")]
+
+
+def cpu_lnv_call(prob, nthreads):
+    """Time one LNV_matrix_multiply(M3, phi, E) call of the oracle's ompGemm chain on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from cq_oracle import OracleSystem
+    from lnv_oracle import OracleLNV, Params
+    os.environ["OMP_NUM_THREADS"] = str(nthreads)
+    import cq_b200
+    rng = cq_b200.lnv_ranges(CFG["rs"], CFG["rh"], CFG["rl"], CFG["rt"])
+    o = OracleSystem(prob["coords"], prob["cell"], np.full(prob["n"], CFG["nsf"]), list(rng.values()))
+    lnv = OracleLNV(o, prob["ridx"], prob["S"], prob["H"], prob["ne_spin"], float(CFG["nsf"] * prob["n"]), Params(),
+                    kernel="ompGemm", nthreads=nthreads)
+    rs = np.random.default_rng(0)
+    lnv.L.v[:] = rs.uniform(-0.01, 0.01, size=lnv.L.v.size)
+    M3 = lnv.temp("L")
+    import cq_oracle
+    cq_oracle._load()
+    t0 = time.perf_counter()
+    lnv.lnv(doM3=True, dophi=True, doE=True, M3=M3, phi=lnv.phi)
+    return time.perf_counter() - t0
+
+
+def flops_of_lnv_call(system, ridx):
+    tot = 0
+    for (t, a, b, c) in lnv_call_products():
+        tot += system.product_work(t, ridx[a], ridx[b], ridx[c])[1]
+    return tot
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def emit(line):
+    print(json.dumps(line), flush=True)
+
+
+def reference_main(args, ws, rank):
+    """CPU arm: the oracle's restatement of the reference's ompGemm chain on all host cores (rank 0 only).
+
+    Each step is one LNV_matrix_multiply(M3, phi, E) call on the workload (a bounded sample of a solve);
+    solves/s = measured flop rate / flops of one solve, with the solve's flop count and the call's flop count
+    taken from the committed work record of the workload (profiles/lnv512_solve_work.json).
+    """
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from cq_b200 import inputs
+    from cq_oracle import OracleSystem
+    from lnv_oracle import OracleLNV, Params
+    import cq_b200
+    rec = json.load(open(work_record_path()))
+    coords, cell = inputs.diamond_si(CFG["ncell"], sigma=CFG["sigma"], seed=CFG["seed"])
+    n = len(coords)
+    rng = cq_b200.lnv_ranges(CFG["rs"], CFG["rh"], CFG["rl"], CFG["rt"])
+    ridx = {k: i for i, k in enumerate(rng)}
+    o = OracleSystem(coords, cell, np.full(n, CFG["nsf"]), list(rng.values()))
+    S = inputs.overlap_S(o.blocklist(ridx["S"], coords, cell))
+    H = inputs.hamiltonian_H(o.blocklist(ridx["H"], coords, cell), seed=CFG["h_seed"])
+    nth = os.cpu_count() or 1
+    lnv = OracleLNV(o, ridx, S, H, CFG["ne_per_atom"] * n / 2.0, float(CFG["nsf"] * n), Params(), kernel="ompGemm",
+                    nthreads=nth)
+    lnv.L.v[:] = np.random.default_rng(0).uniform(-0.01, 0.01, size=lnv.L.v.size)
+    M3 = lnv.temp("L")
+    for _ in range(args.warmup if args.warmup <= 1 else 1):
+        lnv.lnv(doM3=True, dophi=True, doE=True, M3=M3, phi=lnv.phi)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        lnv.lnv(doM3=True, dophi=True, doE=True, M3=M3, phi=lnv.phi)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    value = rec["flops_per_lnv_call"] / t / rec["flops_per_solve"]
+    sample = ("one LNV_matrix_multiply(M3, phi, E) call (9 products, %.3g flop) of the ompGemm restatement per step, "
+              "median %.2f s on %d threads, extrapolated to one solve's %.3g flop" %
+              (rec["flops_per_lnv_call"], t, nth, rec["flops_per_solve"]))
+    emit({"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+          "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+          "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Si supercell, S/H generators)",
+          "config": {"workload": WORKLOAD, "atoms": n, "blocks": "4x4"},
+          "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nth, "kind": "port", "sample": sample},
+          "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return reference_main(args, ws, rank)
+    import torch
+    import cq_b200
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    prob = build_problem(cq_b200)
+    system, solver = prob["system"], prob["solver"]
+    stream = torch.cuda.current_stream()
+    system.set_stream(stream.cuda_stream)
+    dev = torch.device("cuda", local)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # 256 MB > 126 MB L2
+    solver.set_SH(prob["S"], prob["H"])
+    for _ in range(args.warmup):
+        res = solver.solve()
+    torch.cuda.synchronize()
+    # ---- timed region: K solves on device-resident S, H
+    launches0 = system.launch_count()
+    system.profile(True)
+    step_ms = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev_all0, ev_all1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev_all0.record(stream)
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            res = solver.solve()
+            e1.record(stream)
+            step_ms.append((e0, e1))
+        ev_all1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    total_ms = ev_all0.elapsed_time(ev_all1)
+    steps_ms = [a.elapsed_time(b) for a, b in step_ms]
+    prof = system.profile_read()
+    system.profile(False)
+    launches = system.launch_count() - launches0
+    t_max = total_ms
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = ws * args.steps / (t_max / 1e3)
+    # ---- end to end through the host-memory C ABI call (pinned host S, H in; L, K out)
+    pinS = torch.from_numpy(prob["S"]).pin_memory()
+    pinH = torch.from_numpy(prob["H"]).pin_memory()
+    nL = system.length(prob["ridx"]["L"]); nK = system.length(prob["ridx"]["H"])
+    pinL = torch.empty(nL, dtype=torch.float64).pin_memory()
+    pinK = torch.empty(nK, dtype=torch.float64).pin_memory()
+    e2e_steps = max(1, min(args.steps, 3))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        solve_host_pinned(solver, pinS, pinH, pinL, pinK)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = ws * e2e_steps / e2e_s
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        achieved = prof["bytes"] / (prof["ms"] / 1e3) / 1e9 if prof["ms"] > 0 else 0.0
+        traffic = load_traffic()
+        per_solve_flops = res["flops"]
+        fl_call = flops_of_lnv_call(system, prob["ridx"])
+        rec = {"workload": WORKLOAD, "flops_per_solve": per_solve_flops, "products_per_solve": res["n_products"],
+               "flops_per_lnv_call": fl_call, "energy": res["energy"], "electrons": res["electrons"]}
+        os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+        json.dump(rec, open(os.path.join(ROOT, "gpurun_out", "lnv512_solve_work.json"), "w"), indent=1)
+        cpu = None
+        if ws == 1 and not args.no_cpu_baseline:
+            nth = os.cpu_count() or 1
+            t_cpu = cpu_lnv_call(prob, nth)
+            cpu_rate = fl_call / t_cpu
+            cpu = {"value": cpu_rate / per_solve_flops, "unit": "solves/s", "cores": nth, "kind": "port",
+                   "sample": "one LNV_matrix_multiply(M3, phi, E) call (9 products, %.3g flop) of the ompGemm "
+                             "restatement in %.2f s on %d threads, extrapolated to the solve's %.3g flop" %
+                             (fl_call, t_cpu, nth, per_solve_flops)}
+        clocks = clk.summary()
+        srt = sorted(steps_ms)
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Si supercell, S/H generators)",
+            "config": {"workload": WORKLOAD, "atoms": prob["n"], "blocks": "4x4", "ranges_bohr": {"S": 10, "H": 12, "L": 16, "T": 10},
+                       "electrons": int(2 * prob["ne_spin"]), "n_L_iterations": 50, "tolerance": 1e-7,
+                       "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas x%d" % ws},
+            "latency_ms": {"p50": float(np.percentile(srt, 50)), "p99": float(np.percentile(srt, 99))},
+            "solve": {"energy": res["energy"], "electrons": res["electrons"], "products": res["n_products"],
+                      "flops": per_solve_flops, "late_iters": res["late_iters"], "early_iters": res["early_iters"],
+                      "mcw_sweeps": res["mcw_sweeps"], "converged": res["converged"]},
+            "block_mult_tflops": (prof["flops"] / (prof["ms"] / 1e3) / 1e12) if prof["ms"] > 0 else None,
+            "roofline": {"bound": "hbm", "kernel": "k_mult_nd4 (FP64 4x4 block products)", "achieved": achieved,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "launches": prof["launches"],
+                         "avg_launch_ms": prof["ms"] / max(1, prof["launches"]),
+                         "algorithmic_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]),
+                         "share_of_step": prof["ms"] / total_ms if total_ms > 0 else None},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * (prob["S"].size + prob["H"].size),
+                    "d2h_bytes_per_step": 8 * (nL + nK)},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        emit(line)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def solve_host_pinned(solver, pinS, pinH, pinL, pinK):
+    """cq_lnv_solve_host with pinned host buffers: S, H copied in, L and K copied out."""
+    import ctypes
+    import cq_b200
+    r = cq_b200.LNVResult()
+    P = ctypes.POINTER(ctypes.c_double)
+    cq_b200.check(cq_b200.lib().cq_lnv_solve_host(
+        solver._h, ctypes.cast(pinS.data_ptr(), P), ctypes.cast(pinH.data_ptr(), P), ctypes.cast(pinL.data_ptr(), P),
+        ctypes.cast(pinK.data_ptr(), P), ctypes.byref(r)))
+    return r.as_dict()
+
+
+if __name__ == "__main__":
+    main()

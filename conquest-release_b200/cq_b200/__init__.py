@@ -88,6 +88,12 @@ def lib():
         "cq_matrix_trace": [c_void_p, c_int, c_void_p, P(c_double)],
         "cq_matrix_product_trace": [c_void_p, c_int, c_void_p, c_void_p, P(c_double)],
         "cq_synchronize": [c_void_p],
+        "cq_system_set_stream": [c_void_p, c_void_p],
+        "cq_profile_enable": [c_void_p, c_int],
+        "cq_profile_read": [c_void_p, P(c_int64), P(c_double), P(c_double), P(c_double)],
+        "cq_launch_count": [c_void_p, P(c_int64)],
+        "cq_lnv_solve": [c_void_p, P(LNVResult)],
+        "cq_pulay_alphas": [c_int, P(c_double), c_int, c_int, P(c_double)],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -227,6 +233,35 @@ class System:
     def synchronize(self):
         check(lib().cq_synchronize(self._h))
 
+    def set_stream(self, stream):
+        """Enqueue on a cudaStream_t (int handle, e.g. torch.cuda.current_stream().cuda_stream); None = own."""
+        check(lib().cq_system_set_stream(self._h, c_void_p(stream) if stream else None))
+
+    def profile(self, on=True):
+        check(lib().cq_profile_enable(self._h, int(bool(on))))
+
+    def profile_read(self):
+        n, ms, by, fl = c_int64(), c_double(), c_double(), c_double()
+        check(lib().cq_profile_read(self._h, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(by), ctypes.byref(fl)))
+        return {"launches": n.value, "ms": ms.value, "bytes": by.value, "flops": fl.value}
+
+    def launch_count(self):
+        n = c_int64()
+        check(lib().cq_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
+    def blocklist(self, r, coords, cell):
+        """Layout-agnostic description of range r (global atoms, images, radii, offsets) for the input generators."""
+        from .inputs import BlockList
+        nnab = self.geti("n_nab", r)
+        ig_prim = self.geti("ig_prim") - 1
+        ig_j = self.geti("ig_j", r) - 1
+        shift = self.geti("shift", r).reshape(-1, 3)
+        nd_i = np.repeat(self.geti("ndimi", r), nnab)
+        nd_j = self.geti("ndimj", r)
+        elem = self.geti("elem", r)
+        return BlockList(np.repeat(ig_prim, nnab), ig_j, shift, self.radius(r), nd_i, nd_j, elem, self.length(r))
+
 
 def m_kern(kind, k_off, kpart, ib_nd_acc, ibaddr, nbnab, ibpart, ibseq, bndim2, a, b, c, ahalo, chalo, at,
            mx_absb=0, mx_part=0, mx_iprim=0):
@@ -292,6 +327,12 @@ class LNV:
         check(lib().cq_lnv_invert_S(self._h, ctypes.byref(w)))
         return w.value
 
+    def solve(self):
+        """T = S^-1 and FindMinDM from the McWeeny start on the device-resident S and H."""
+        r = LNVResult()
+        check(lib().cq_lnv_solve(self._h, ctypes.byref(r)))
+        return r.as_dict()
+
     def find_min_dm(self, resetL=True):
         r = LNVResult()
         check(lib().cq_lnv_find_min_dm(self._h, int(bool(resetL)), ctypes.byref(r)))
@@ -315,3 +356,13 @@ class LNV:
         check(lib().cq_lnv_solve_host(self._h, _dp(S), _dp(H), _dp(Lo) if Lo is not None else None,
                                       _dp(Ko) if Ko is not None else None, ctypes.byref(r)))
         return r.as_dict(), Lo, Ko
+
+
+def pulay_alphas(ipulay, Aij, n, max_n):
+    """DoPulay2D_nospin mixing coefficients (host computation in libcqb200.so)."""
+    A = np.zeros((max_n, max_n))
+    A[:n, :n] = np.asarray(Aij)[:n, :n]
+    Af = np.asfortranarray(A)
+    al = np.zeros(max_n)
+    check(lib().cq_pulay_alphas(int(ipulay), Af.ctypes.data_as(P(c_double)), int(n), int(max_n), _dp(al)))
+    return al

@@ -8,6 +8,10 @@
 // Elementwise kernels are HBM-bound grid-stride loops with 16-byte accesses;
 // the reductions are two-level with a fixed grid, so results are identical
 // from run to run.
+#include <climits>
+#include <cmath>
+#include <limits>
+
 #include "cq_internal.hpp"
 
 namespace cqb {
@@ -58,51 +62,108 @@ __global__ void k_transpose(int nnz, const int* __restrict__ dest, const int64_t
     T[n2 + ndj * n1] = A[t];
   }
 }
-// deterministic dot product: fixed-grid partials, then one block sums them in order
-__global__ void k_dot_partial(const double* __restrict__ x, const double* __restrict__ y, int64_t n, double* __restrict__ part) {
-  __shared__ double s[kT];
-  double acc = 0.0;
+// ---------------------------------------------------------------------------
+// Exact, order-independent sums (matrix_product_trace / matrix_trace).
+// Every term (a rounded product x*y, or an element) is converted exactly to a
+// 192-bit two's-complement fixed-point integer whose least significant bit is
+// 2^(emax-150), emax being the largest binary exponent among the terms (pass 1).
+// Integer addition is associative, so the sum does not depend on the grid or on
+// the order of the terms; the host rounds it once to the nearest double.
+// Terms below 2^(emax-150) are truncated toward zero (relative effect < n 2^-150).
+// ---------------------------------------------------------------------------
+constexpr int kAccFrac = 150;   // fraction bits kept below the largest term's exponent
+
+struct Acc192 { uint64_t w[3]; };
+
+__device__ __forceinline__ void acc_add(Acc192& a, const Acc192& b) {
+  uint64_t s0 = a.w[0] + b.w[0];
+  uint64_t c0 = s0 < a.w[0];
+  uint64_t s1 = a.w[1] + b.w[1];
+  uint64_t c1 = s1 < a.w[1];
+  uint64_t s1c = s1 + c0;
+  c1 += s1c < s1;
+  a.w[0] = s0; a.w[1] = s1c; a.w[2] = a.w[2] + b.w[2] + c1;
+}
+// term v -> fixed point with lsb 2^lsb_exp (exact for every bit at or above the lsb)
+__device__ __forceinline__ void acc_term(Acc192& a, double v, int lsb_exp) {
+  if (v == 0.0) return;
+  int e;
+  double f = frexp(v, &e);                              // v = f 2^e, 0.5 <= |f| < 1
+  long long m = (long long)ldexp(f, 53);                // exact, |m| < 2^53
+  bool neg = m < 0;
+  uint64_t mag = (uint64_t)(neg ? -m : m);
+  int s = e - 53 - lsb_exp;                             // bit position of m's lsb
+  Acc192 t = {{0, 0, 0}};
+  if (s >= 0) {
+    int idx = s >> 6, off = s & 63;
+    if (idx < 3) t.w[idx] = mag << off;
+    if (off && idx + 1 < 3) t.w[idx + 1] = mag >> (64 - off);
+  } else if (-s < 64) {
+    t.w[0] = mag >> (-s);
+  }
+  if (neg) {                                            // two's complement negation
+    t.w[0] = ~t.w[0]; t.w[1] = ~t.w[1]; t.w[2] = ~t.w[2];
+    Acc192 one = {{1, 0, 0}};
+    acc_add(t, one);
+  }
+  acc_add(a, t);
+}
+__device__ __forceinline__ double dterm(const double* x, const double* y, int64_t i) {
+  return y ? __dmul_rn(x[i], y[i]) : x[i];
+}
+// pass 1: largest exponent of the nonzero terms; a non-finite term sets the flag
+__global__ void k_acc_emax(const double* __restrict__ x, const double* __restrict__ y, int64_t n, int* __restrict__ emax,
+                           int* __restrict__ nonfinite) {
+  int best = INT_MIN;
+  bool bad = false;
+  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT) {
+    double v = dterm(x, y, i);
+    if (!isfinite(v)) { bad = true; continue; }
+    if (v != 0.0) { int e; frexp(v, &e); best = max(best, e); }
+  }
+  for (int o = 16; o; o >>= 1) best = max(best, __shfl_down_sync(0xffffffffu, best, o));
+  if ((threadIdx.x & 31) == 0 && best != INT_MIN) atomicMax(emax, best);
+  if (bad) atomicExch(nonfinite, 1);
+}
+__device__ void block_acc_reduce(Acc192 a, uint64_t* __restrict__ out) {
+  __shared__ uint64_t s[3][kT];
+  for (int k = 0; k < 3; ++k) s[k][threadIdx.x] = a.w[k];
+  __syncthreads();
+  for (int w = kT / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      Acc192 x = {{s[0][threadIdx.x], s[1][threadIdx.x], s[2][threadIdx.x]}};
+      Acc192 z = {{s[0][threadIdx.x + w], s[1][threadIdx.x + w], s[2][threadIdx.x + w]}};
+      acc_add(x, z);
+      for (int k = 0; k < 3; ++k) s[k][threadIdx.x] = x.w[k];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) for (int k = 0; k < 3; ++k) out[k] = s[k][0];
+}
+// pass 2: fixed-point accumulation, one 192-bit partial per block
+__global__ void __launch_bounds__(kT) k_acc_sum(const double* __restrict__ x, const double* __restrict__ y, int64_t n,
+                                                const int* __restrict__ emax, uint64_t* __restrict__ part) {
+  Acc192 a = {{0, 0, 0}};
+  const int lsb = *emax - kAccFrac;
   for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT)
-    acc = fma(x[i], y[i], acc);
-  s[threadIdx.x] = acc;
-  __syncthreads();
-  for (int w = kT / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+    acc_term(a, dterm(x, y, i), lsb);
+  block_acc_reduce(a, part + 3 * blockIdx.x);
 }
-__global__ void k_sum_final(const double* __restrict__ part, int n, double* __restrict__ out) {
-  __shared__ double s[kT];
-  double acc = 0.0;
-  for (int i = threadIdx.x; i < n; i += kT) acc += part[i];
-  s[threadIdx.x] = acc;
-  __syncthreads();
-  for (int w = kT / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
-    __syncthreads();
+__global__ void __launch_bounds__(kT) k_acc_final(const uint64_t* __restrict__ part, int nb, uint64_t* __restrict__ out) {
+  Acc192 a = {{0, 0, 0}};
+  for (int b = threadIdx.x; b < nb; b += kT) {
+    Acc192 t = {{part[3 * b], part[3 * b + 1], part[3 * b + 2]}};
+    acc_add(a, t);
   }
-  if (threadIdx.x == 0) *out = s[0];
+  block_acc_reduce(a, out);
 }
-// onsite diagonal sum: sequential over primary atoms inside one block (n_prim is small)
-__global__ void k_trace(int n_prim, const int64_t* __restrict__ onsite, const int* __restrict__ prim_nsf,
-                        const double* __restrict__ a, double* __restrict__ out) {
-  __shared__ double s[kT];
-  double acc = 0.0;
-  for (int p = threadIdx.x; p < n_prim; p += kT) {
-    int nd = prim_nsf[p];
-    const double* A = a + onsite[p];
-    double t = 0.0;
-    for (int j = 0; j < nd; ++j) t += A[j * nd + j];
-    acc += t;
-  }
-  s[threadIdx.x] = acc;
-  __syncthreads();
-  for (int w = kT / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *out = s[0];
+// onsite diagonal elements gathered for the exact trace
+__global__ void k_gather_diag(int n_prim, const int64_t* __restrict__ onsite, const int* __restrict__ prim_nsf,
+                              const int* __restrict__ diag_off, const double* __restrict__ a, double* __restrict__ out) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_prim) return;
+  int nd = prim_nsf[p];
+  for (int j = 0; j < nd; ++j) out[diag_off[p] + j] = a[onsite[p] + j * nd + j];
 }
 // GetHLimits: per primary atom and column orbital i, HMin_i = sum(+-|H|), HMax_i = sum |H|
 // (onsite block adds |H| to both); min/max over atoms are order independent.
@@ -147,27 +208,18 @@ __global__ void k_minmax(const double* __restrict__ mn, const double* __restrict
   if (threadIdx.x == 0) { out[0] = smn[0]; out[1] = smx[0]; }
 }
 
-double fetch_scalar(System& S, const double* d) {
-  double h = 0.0;
-  CQ_CUDA(cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, S.stream));
-  CQ_CUDA(cudaStreamSynchronize(S.stream));
-  return h;
-}
-
-void ensure_scratch(System& S) {
-  if (S.red_scratch.n < (size_t)kRedBlocks + 8) S.red_scratch.alloc(kRedBlocks + 8);
-}
-
 }  // namespace
 
 void dev_scale(System& S, double* a, int64_t n, double alpha) {
   if (n <= 0) return;
   k_scale<<<grid_for(n), kT, 0, S.stream>>>(a, n, alpha);
+  S.launches++;
   CQ_CUDA(cudaGetLastError());
 }
 void dev_axpy(System& S, double* a, int64_t n, double beta, const double* b) {
   if (n <= 0) return;
   k_axpy<<<grid_for(n), kT, 0, S.stream>>>(a, n, beta, b);
+  S.launches++;
   CQ_CUDA(cudaGetLastError());
 }
 void dev_copy(System& S, double* dst, const double* src, int64_t n) {
@@ -181,6 +233,7 @@ void dev_matrix_add(System& S, int ra, double* a, double alpha, int rb, const do
   k_masked_add<<<(int)(((int64_t)A.nnz * 32 + kT - 1) / kT), kT, 0, S.stream>>>(
       A.nnz, m.partner.p, A.nb_elem.p, B.nb_elem.p, A.nb_row.p, A.nb_cover.p, S.dg.prim_nsf.p, S.dg.cover_nsf.p, a, alpha,
       b, beta);
+  S.launches++;
   CQ_CUDA(cudaGetLastError());
 }
 void dev_transpose(System& S, int r, const double* a, double* at) {
@@ -189,21 +242,71 @@ void dev_transpose(System& S, int r, const double* a, double* at) {
   if (R.nnz == 0) return;
   k_transpose<<<(int)(((int64_t)R.nnz * 32 + kT - 1) / kT), kT, 0, S.stream>>>(
       R.nnz, R.trans_dest.p, R.nb_elem.p, R.nb_row.p, R.nb_cover.p, S.dg.prim_nsf.p, S.dg.cover_nsf.p, a, at);
+  S.launches++;
   CQ_CUDA(cudaGetLastError());
 }
-double dev_dot(System& S, const double* x, const double* y, int64_t n) {
-  ensure_scratch(S);
-  k_dot_partial<<<kRedBlocks, kT, 0, S.stream>>>(x, y, n, S.red_scratch.p);
-  k_sum_final<<<1, kT, 0, S.stream>>>(S.red_scratch.p, kRedBlocks, S.red_scratch.p + kRedBlocks);
-  CQ_CUDA(cudaGetLastError());
-  return fetch_scalar(S, S.red_scratch.p + kRedBlocks);
+// Round a 192-bit two's-complement fixed-point value (lsb = 2^lsb_exp) to the nearest double, ties to even.
+double acc192_to_double(const uint64_t in[3], int lsb_exp) {
+  uint64_t w[3] = {in[0], in[1], in[2]};
+  bool neg = (w[2] >> 63) != 0;
+  if (neg) {
+    w[0] = ~w[0]; w[1] = ~w[1]; w[2] = ~w[2];
+    if (++w[0] == 0 && ++w[1] == 0) ++w[2];
+  }
+  int h = -1;
+  for (int k = 2; k >= 0 && h < 0; --k)
+    if (w[k]) h = 64 * k + 63 - __builtin_clzll(w[k]);
+  if (h < 0) return 0.0;
+  auto bit = [&](int b) -> uint64_t { return b < 0 ? 0 : (w[b >> 6] >> (b & 63)) & 1u; };
+  uint64_t m = 0;
+  int sh = h > 52 ? h - 52 : 0;                  // bits dropped below the 53-bit mantissa
+  for (int b = h; b >= sh; --b) m = (m << 1) | bit(b);
+  if (sh > 0) {
+    uint64_t half = bit(sh - 1), sticky = 0;
+    for (int b = sh - 2; b >= 0 && !sticky; --b) sticky |= bit(b);
+    if (half && (sticky || (m & 1))) ++m;         // may carry to 2^53, still exact in a double
+  }
+  double v = std::ldexp((double)m, lsb_exp + sh);
+  return neg ? -v : v;
 }
+
+static double exact_sum(System& S, const double* x, const double* y, int64_t n) {
+  if (S.acc_part.n < (size_t)(3 * kRedBlocks + 3)) S.acc_part.alloc(3 * kRedBlocks + 3);
+  if (S.acc_flags.n < 2) S.acc_flags.alloc(2);
+  int init[2] = {INT_MIN, 0};
+  CQ_CUDA(cudaMemcpyAsync(S.acc_flags.p, init, sizeof(init), cudaMemcpyHostToDevice, S.stream));
+  k_acc_emax<<<kRedBlocks, kT, 0, S.stream>>>(x, y, n, S.acc_flags.p, S.acc_flags.p + 1);
+  int flags[2];
+  CQ_CUDA(cudaMemcpyAsync(flags, S.acc_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, S.stream));
+  CQ_CUDA(cudaStreamSynchronize(S.stream));
+  S.launches++;
+  if (flags[1]) return std::numeric_limits<double>::quiet_NaN();
+  if (flags[0] == INT_MIN) return 0.0;
+  k_acc_sum<<<kRedBlocks, kT, 0, S.stream>>>(x, y, n, S.acc_flags.p, S.acc_part.p);
+  k_acc_final<<<1, kT, 0, S.stream>>>(S.acc_part.p, kRedBlocks, S.acc_part.p + 3 * kRedBlocks);
+  S.launches += 2;
+  CQ_CUDA(cudaGetLastError());
+  uint64_t w[3];
+  CQ_CUDA(cudaMemcpyAsync(w, S.acc_part.p + 3 * kRedBlocks, sizeof(w), cudaMemcpyDeviceToHost, S.stream));
+  CQ_CUDA(cudaStreamSynchronize(S.stream));
+  return acc192_to_double(w, flags[0] - kAccFrac);
+}
+
+double dev_dot(System& S, const double* x, const double* y, int64_t n) { return exact_sum(S, x, y, n); }
+
 double dev_trace(System& S, int r, const double* a) {
-  ensure_scratch(S);
   RangeIndex& R = *S.ranges[r];
-  k_trace<<<1, kT, 0, S.stream>>>(S.geo.n_prim, R.onsite.p, S.dg.prim_nsf.p, a, S.red_scratch.p + kRedBlocks);
+  const int N = S.geo.n_prim;
+  if (S.diag_off.n == 0) {
+    std::vector<int> off(N + 1, 0);
+    for (int p = 0; p < N; ++p) off[p + 1] = off[p] + S.geo.nsf[S.geo.prim_global[p]];
+    S.diag_off.upload(off, S.stream);
+    S.diag_buf.alloc(std::max(off[N], 1));
+  }
+  k_gather_diag<<<(N + kT - 1) / kT, kT, 0, S.stream>>>(N, R.onsite.p, S.dg.prim_nsf.p, S.diag_off.p, a, S.diag_buf.p);
+  S.launches++;
   CQ_CUDA(cudaGetLastError());
-  return fetch_scalar(S, S.red_scratch.p + kRedBlocks);
+  return exact_sum(S, S.diag_buf.p, nullptr, (int64_t)S.diag_buf.n);
 }
 void dev_h_limits(System& S, int r, const double* h, double* hmin, double* hmax) {
   RangeIndex& R = *S.ranges[r];
@@ -213,6 +316,7 @@ void dev_h_limits(System& S, int r, const double* h, double* hmin, double* hmax)
   k_hlimits<<<(N * 32 + kT - 1) / kT, kT, 0, S.stream>>>(N, R.row_ptr.p, R.nb_elem.p, R.nb_cover.p, R.onsite.p,
                                                        S.dg.prim_nsf.p, S.dg.cover_nsf.p, h, mn.p, mx.p);
   k_minmax<<<1, kT, 0, S.stream>>>(mn.p, mx.p, N, out.p);
+  S.launches += 2;
   CQ_CUDA(cudaGetLastError());
   double o[2];
   CQ_CUDA(cudaMemcpyAsync(o, out.p, sizeof(o), cudaMemcpyDeviceToHost, S.stream));

@@ -16,7 +16,7 @@ System::~System() {
   plans.clear();
   addmaps.clear();
   ranges.clear();
-  if (own_stream && stream) cudaStreamDestroy(stream);
+  if (own_stream && own) cudaStreamDestroy(own);
 }
 
 // drop-in kernels (one m_kern_max / m_kern_min call): explicit offsets prepared on the host
@@ -79,6 +79,7 @@ int cq_system_create(int n_atoms, const double* coords, const double* cell, cons
     auto sys = std::make_unique<cq_system>();
     System& S = sys->S;
     CQ_CUDA(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
+    S.own = S.stream;
     S.own_stream = true;
     GeometryParams prm;
     prm.max_atoms_part = max_atoms_part > 0 ? max_atoms_part : 34;
@@ -208,6 +209,44 @@ int cq_matrix_product_trace(cq_system* sys, int r, const double* a_dev, const do
 
 int cq_synchronize(cq_system* sys) {
   return guarded([&] { check_sys(sys); CQ_CUDA(cudaStreamSynchronize(sys->S.stream)); });
+}
+
+int cq_system_set_stream(cq_system* sys, void* stream) {
+  return guarded([&] {
+    check_sys(sys);
+    CQ_CUDA(cudaStreamSynchronize(sys->S.stream));
+    sys->S.stream = stream ? (cudaStream_t)stream : sys->S.own;
+  });
+}
+
+int cq_profile_enable(cq_system* sys, int on) {
+  return guarded([&] {
+    check_sys(sys);
+    sys->S.prof.on = on != 0;
+    sys->S.prof.clear();
+  });
+}
+
+int cq_profile_read(cq_system* sys, int64_t* launches, double* ms, double* bytes, double* flops) {
+  return guarded([&] {
+    check_sys(sys);
+    CQ_CUDA(cudaStreamSynchronize(sys->S.stream));
+    double t = 0, by = 0, fl = 0;
+    for (auto& r : sys->S.prof.recs) {
+      float e = 0.f;
+      CQ_CUDA(cudaEventElapsedTime(&e, r.a, r.b));
+      t += e; by += r.bytes; fl += r.flops;
+    }
+    if (launches) *launches = (int64_t)sys->S.prof.recs.size();
+    if (ms) *ms = t;
+    if (bytes) *bytes = by;
+    if (flops) *flops = fl;
+    sys->S.prof.clear();
+  });
+}
+
+int cq_launch_count(cq_system* sys, int64_t* count) {
+  return guarded([&] { check_sys(sys); CQ_CHECK(count, CQ_ERR_ARG, "null argument"); *count = sys->S.launches; });
 }
 
 // ---------------------------------------------------------------------------

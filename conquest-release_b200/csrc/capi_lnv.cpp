@@ -138,6 +138,25 @@ int cq_lnv_put(cq_lnv* s, const char* name, const double* in, int on_device) {
   });
 }
 
+int cq_pulay_alphas(int ipulay, const double* Aij, int n, int max_n, double* alphas) {
+  return guarded_call([&] {
+    CQ_CHECK(Aij && alphas && n >= 1 && n <= max_n && ipulay >= 1 && ipulay <= max_n, CQ_ERR_ARG, "bad Pulay arguments");
+    LNVSolver::do_pulay(ipulay, Aij, n, max_n, alphas);
+  });
+}
+
+int cq_lnv_solve(cq_lnv* s, cq_lnv_result* res) {
+  return guarded_call([&] {
+    CQ_CHECK(s, CQ_ERR_ARG, "null argument");
+    LNVSolver& L = *s->solver;
+    L.stats = LNVStats();
+    L.invert_S();
+    L.delta_e = 0.0;
+    L.find_min_dm(true);
+    fill_result(L.stats, res);
+  });
+}
+
 int cq_lnv_solve_host(cq_lnv* s, const double* S, const double* H, double* L_out, double* K_out, cq_lnv_result* res) {
   return guarded_call([&] {
     CQ_CHECK(s && S && H, CQ_ERR_ARG, "null argument");

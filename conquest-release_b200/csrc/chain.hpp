@@ -64,6 +64,7 @@ class LNVSolver {
 
   double invert_S();
   void find_min_dm(bool resetL);
+  static void do_pulay(int iPulay, const double* Aij, int n, int max_n, double* al);
   void lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim, double* electrons, double* energy);
 
  private:
@@ -94,7 +95,6 @@ class LNVSolver {
   void project_gradient(DMat& M3, DMat& SM3, DMat& Sphi, DMat& mtemp);
   int early_dm(int ndone, bool& inflex);
   int late_dm(int ndone, bool& done, double& deltaE);
-  static void do_pulay(int iPulay, const double* Aij, int n, int max_n, double* al);
 };
 
 }  // namespace cqb

@@ -115,6 +115,7 @@ struct Geometry {
   std::vector<int> cover_first;       // [np] first cover atom (0-based)
   std::vector<int> cover_count;       // [np]
   std::vector<int> label_to_cover;    // [label] -> np (0-based), -1 if none
+  std::vector<int> cover_shift;       // [3*np] periodic image of the partition, in cell vectors
   std::vector<double> cover_x;        // [3c]
   std::vector<int> cover_global;      // [c] input atom
   std::vector<int> cover_part;        // [c] cover partition np
@@ -182,6 +183,17 @@ struct AddMap {                   // partner of each block of range A in range B
   DevBuf<int> partner;
 };
 
+// CUDA-event timing of the block-product launches (enabled on request)
+struct ProductProfile {
+  bool on = false;
+  struct Rec { cudaEvent_t a, b; double bytes, flops; };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> spare;
+  cudaEvent_t get();
+  void clear();
+  ~ProductProfile();
+};
+
 struct System {
   Geometry geo;
   DevGeometry dg;
@@ -189,9 +201,16 @@ struct System {
   std::map<std::tuple<int, int, int, int>, std::unique_ptr<ProductPlan>> plans;
   std::map<std::pair<int, int>, std::unique_ptr<AddMap>> addmaps;
   cudaStream_t stream = nullptr;
+  cudaStream_t own = nullptr;     // the stream created with the system
   bool own_stream = false;
   int uniform_nsf = 0;            // block size when every atom has the same one, else 0
-  DevBuf<double> red_scratch;     // partial sums of the deterministic reductions
+  DevBuf<double> red_scratch;     // scratch of the min/max reductions
+  DevBuf<uint64_t> acc_part;      // 192-bit partials of the exact sums
+  DevBuf<int> acc_flags;          // largest exponent, non-finite flag
+  DevBuf<int> diag_off;           // first onsite-diagonal slot of each primary atom
+  DevBuf<double> diag_buf;        // gathered onsite diagonal (exact trace)
+  int64_t launches = 0;           // kernels launched by this system (all kinds)
+  ProductProfile prof;
   ~System();
 };
 

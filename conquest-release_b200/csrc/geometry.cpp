@@ -413,6 +413,7 @@ void build_geometry(Geometry& g, int n, const double* coords, const double* cell
   g.cover_first.assign(g.ng_cover + 1, 0); g.cover_count.assign(g.ng_cover, 0);
   g.label_to_cover.assign(g.ng_cover + 1, -1);
   g.cover_x.clear(); g.cover_global.clear(); g.cover_part.clear(); g.cover_seq.clear(); g.cover_nsf.clear();
+  g.cover_shift.clear();
   for (int np_ = 0; np_ < g.ng_cover; ++np_) {
     int q[3];
     double add[3];
@@ -421,6 +422,7 @@ void build_geometry(Geometry& g, int n, const double* coords, const double* cell
       add[d] = (double)(co[d] + off[np_][d] - q[d]) * (g.cell[d] / (double)g.n_parts[d]);
     }
     int cc = ((q[0] - 1) * g.n_parts[1] + (q[1] - 1)) * g.n_parts[2] + q[2];
+    for (int d = 0; d < 3; ++d) g.cover_shift.push_back((co[d] + off[np_][d] - q[d]) / g.n_parts[d]);
     g.cover_cell[np_] = cc;
     g.cover_label[np_] = ((off[np_][0] + span[0]) * ncov[1] + (off[np_][1] + span[1])) * ncov[2] + (off[np_][2] + span[2]) + 1;
     g.label_to_cover[g.cover_label[np_]] = np_;

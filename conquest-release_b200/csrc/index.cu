@@ -607,7 +607,11 @@ void export_range_array(System& S, int r, const std::string& nm, std::vector<int
   std::vector<int> part_of_row(N), first_row_of_part(g.np_in_cell + 1);
   for (int q = 0; q <= g.np_in_cell; ++q) first_row_of_part[q] = g.part_first_prim[q];
   for (int p = 0; p < N; ++p) part_of_row[p] = g.prim_part[p];
-  if (nm == "n_nab") { for (int p = 0; p < N; ++p) v.push_back(rp[p + 1] - rp[p]); }
+  if (nm == "shift") {  // image of each stored neighbour, in cell vectors (3 per block)
+    for (int e = 0; e < R.nnz; ++e) for (int d = 0; d < 3; ++d) v.push_back(g.cover_shift[3 * g.cover_part[cov[e]] + d]);
+  } else if (nm == "ig_j") { for (int e = 0; e < R.nnz; ++e) v.push_back(g.cover_global[cov[e]] + 1); }
+  else if (nm == "elem") { for (int e = 0; e < R.nnz; ++e) v.push_back(el[e]); }
+  else if (nm == "n_nab") { for (int p = 0; p < N; ++p) v.push_back(rp[p + 1] - rp[p]); }
   else if (nm == "i_acc") { for (int p = 0; p < N; ++p) v.push_back(rp[p] + 1); }
   else if (nm == "i_nd_acc") {
     for (int p = 0; p < N; ++p) v.push_back(rp[p + 1] > rp[p] ? el[rp[p]] + 1 : 0);

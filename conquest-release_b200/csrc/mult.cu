@@ -192,6 +192,9 @@ void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, doub
   if (M.n_out == 0) return;
   cudaStream_t st = S.stream;
   const int T = 256;
+  cudaEvent_t ev0 = nullptr;
+  if (S.prof.on) { ev0 = S.prof.get(); CQ_CUDA(cudaEventRecord(ev0, st)); }
+  S.launches++;
   // the 4 x 4 path reads B with 16-byte vector loads: require 16-byte aligned operands
   bool aligned = ((uintptr_t)b % 16 == 0) && ((uintptr_t)M.x % 16 == 0);
   if (S.uniform_nsf == 4 && aligned) {
@@ -210,6 +213,28 @@ void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, doub
     }
   }
   CQ_CUDA(cudaGetLastError());
+  if (S.prof.on) {
+    cudaEvent_t ev1 = S.prof.get();
+    CQ_CUDA(cudaEventRecord(ev1, st));
+    // algorithmic bytes: read both operands once, write the result once (8 bytes per element)
+    double bytes = 8.0 * (double)(A.length + B.length + C.length);
+    S.prof.recs.push_back({ev0, ev1, bytes, (double)P.flops});
+  }
+}
+
+cudaEvent_t ProductProfile::get() {
+  if (!spare.empty()) { cudaEvent_t e = spare.back(); spare.pop_back(); return e; }
+  cudaEvent_t e;
+  CQ_CUDA(cudaEventCreate(&e));
+  return e;
+}
+void ProductProfile::clear() {
+  for (auto& r : recs) { spare.push_back(r.a); spare.push_back(r.b); }
+  recs.clear();
+}
+ProductProfile::~ProductProfile() {
+  clear();
+  for (cudaEvent_t e : spare) cudaEventDestroy(e);
 }
 
 }  // namespace cqb

@@ -144,6 +144,17 @@ int cq_matrix_product_trace(cq_system* sys, int r, const double* a_dev, const do
 /* Synchronise the system's stream. */
 int cq_synchronize(cq_system* sys);
 
+/* Enqueue all further work of the system on `stream` (a cudaStream_t); NULL restores its own stream. */
+int cq_system_set_stream(cq_system* sys, void* stream);
+
+/* CUDA-event timing of every block-product launch (timer_module's tmr_std_matmult, per launch). */
+int cq_profile_enable(cq_system* sys, int on);
+/* Synchronise, return and reset: timed product launches, their total milliseconds, algorithmic
+ * bytes (8 * (len A + len B + len C) per launch) and flops (2 sum nd^3 over the triples). */
+int cq_profile_read(cq_system* sys, int64_t* launches, double* ms, double* bytes, double* flops);
+/* Kernels launched by this system so far (all kinds). */
+int cq_launch_count(cq_system* sys, int64_t* count);
+
 /* ------------------------------------------------------------------------ */
 /* LNV / McWeeny density-matrix minimisation (one spin channel, nspin = 1)   */
 /* ------------------------------------------------------------------------ */
@@ -197,6 +208,16 @@ int cq_lnv_find_min_dm(cq_lnv* s, int resetL, cq_lnv_result* res);
 int cq_lnv_get(cq_lnv* s, const char* name, double* out, int64_t cap, int on_device);
 /* Copy a matrix in (for example a previous L): name in "L", "T". */
 int cq_lnv_put(cq_lnv* s, const char* name, const double* in, int on_device);
+/*
+ * DoPulay2D_nospin (src/Pulay.f90:188-262): Pulay mixing coefficients from the
+ * n x n residual overlap Aij (column major, leading dimension max_n), inverted by
+ * Bunch-Kaufman pivoting as LAPACK dsytf2/dsytri; if a pivot is singular alphas is
+ * the unit vector e_ipulay.  Host-only, needs no GPU.
+ */
+int cq_pulay_alphas(int ipulay, const double* Aij, int n, int max_n, double* alphas);
+
+/* One complete solve on the device-resident S and H: T = S^-1, then FindMinDM from the McWeeny start. */
+int cq_lnv_solve(cq_lnv* s, cq_lnv_result* res);
 /*
  * One complete solve from host arrays: load S and H, T = S^-1, FindMinDM from
  * the McWeeny start, copy L and K back (either may be NULL).  This is the

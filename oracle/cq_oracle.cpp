@@ -1036,6 +1036,56 @@ static void m_kern_min_default(const KernArgs& K) {
   }
 }
 
+// m_kern_max / m_kern_min, ompDoii kernel (multiply_kernel_ompDoii.f90:132-262 and its m_kern_min):
+// the default kernel's arithmetic with `!$omp do` over the primary neighbours i of each k.
+// Different i write different output blocks, so every element sees the default kernel's
+// operation sequence: results are bit-identical to the default kernel for any thread count.
+static void m_kern_doii(const KernArgs& K, int type) {
+  const Halo& ah = *K.ahalo; const Halo& ch = *K.chalo; const Trans& at = *K.at;
+  for (int k = 1; k <= ah.nh_part[K.kpart]; ++k) {
+    int k_in_halo = ah.j_beg[K.kpart] + k - 1;
+    int k_in_part = ah.j_seq[k_in_halo];
+    int nbkbeg = K.ibaddr[k_in_part];
+    int nb_nd_kbeg = K.ib_nd_acc[k_in_part];
+    int nd3 = ah.ndimj[k_in_halo];
+    int nhn = at.n_hnab[k_in_halo];
+    int nbn = K.nbnab[k_in_part];
+    vector<int> nd1_1st(nhn + 2, 0), nd2_1st(nbn + 2, 0), jbnab2ch(nbn + 1, 0);
+    for (int i = 2; i <= nhn; ++i) nd1_1st[i] = nd1_1st[i - 1] + nd3 * ah.ndimi[at.i_prim[at.i_beg[k_in_halo] + i - 2]];
+    for (int j = 2; j <= nbn; ++j) nd2_1st[j] = nd2_1st[j - 1] + nd3 * K.bndim2[nbkbeg + j - 2];
+    for (int j = 1; j <= nbn; ++j) {
+      int jpart = K.ibpart[nbkbeg + j - 1] + K.k_off;
+      jbnab2ch[j] = ch.i_halo[ch.i_hbeg[jpart] + K.ibseq[nbkbeg + j - 1] - 1];
+    }
+#pragma omp for schedule(runtime)
+    for (int i = 1; i <= nhn; ++i) {
+      int i_in_prim = at.i_prim[at.i_beg[k_in_halo] + i - 1];
+      int nd1 = ah.ndimi[i_in_prim];
+      size_t icad = (size_t)(i_in_prim - 1) * ch.ni_in_halo;
+      int nabeg = at.i_nd_beg[k_in_halo] + nd1_1st[i];
+      for (int j = 1; j <= nbn; ++j) {
+        int nd2 = K.bndim2[nbkbeg + j - 1];
+        int nbbeg = nb_nd_kbeg + nd2_1st[j];
+        int jh = jbnab2ch[j];
+        if (jh == 0) continue;
+        int ncbeg = (int)ch.i_h2d[icad + jh];
+        if (ncbeg == 0) continue;
+        for (int n2 = 1; n2 <= nd2; ++n2) {
+          int nbaddr = nbbeg + nd3 * (n2 - 1);
+          int ncaddr = ncbeg + nd1 * (n2 - 1);
+          for (int n1 = 1; n1 <= nd1; ++n1) {
+            int naaddr = nabeg + nd3 * (n1 - 1);
+            for (int n3 = 1; n3 <= nd3; ++n3) {
+              if (type == 1) K.c[ncaddr + n1 - 1] = K.c[ncaddr + n1 - 1] + K.a[naaddr + n3 - 1] * K.b[nbaddr + n3 - 1];
+              else K.a[naaddr + n3 - 1] = K.a[naaddr + n3 - 1] + K.c[ncaddr + n1 - 1] * K.b[nbaddr + n3 - 1];
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
 // scipy's bundled OpenBLAS dgemm (Fortran ABI), resolved at load time by the Python side
 typedef void (*dgemm_fn)(const char*, const char*, const int*, const int*, const int*, const double*, const double*,
                          const int*, const double*, const int*, const double*, double*, const int*);
@@ -1187,7 +1237,7 @@ static void mat_mult(System& s, int mult_type, int ra, int rb, int rc, double* a
   vector<int> ibpart_rem;
   int n_cont = 0, ilen2 = 0;
 #ifdef _OPENMP
-  if (kernel == 1 && nthreads > 0) omp_set_num_threads(nthreads);
+  if (kernel != 0 && nthreads > 0) omp_set_num_threads(nthreads);
 #endif
   int kpart_shared = 0, k_off_shared = 0;
   auto prefetch_part = [&](int kpart) {
@@ -1251,7 +1301,9 @@ static void mat_mult(System& s, int mult_type, int ra, int rb, int rc, double* a
         }
 #pragma omp barrier
         KernArgs K = make_args(kpart_shared, k_off_shared);
-        if (mult_type == 1) m_kern_max_ompgemm(K); else m_kern_min_ompgemm(K);
+        if (kernel == 2) m_kern_doii(K, mult_type);
+        else if (mult_type == 1) m_kern_max_ompgemm(K);
+        else m_kern_min_ompgemm(K);
 #pragma omp barrier
       }
     }
@@ -1478,13 +1530,15 @@ double orc_matrix_trace(void* h, int r, const double* a0) {
   System& s = *(System*)h;
   Range& R = s.ranges[r];
   const double* a = a0 - 1;
-  double tr = 0.0;
+  std::vector<double> diag;
   for (int np_ = 1; np_ <= s.groups_on_node; ++np_)
     for (int i = 1; i <= s.nm_nodgroup[np_]; ++i) {
       int sf1 = R.mat[np_].ndimi[i];
-      for (int j = 1; j <= sf1; ++j) tr += a[(j - 1) * sf1 + j - 1 + R.mat[np_].onsite[i]];
+      for (int j = 1; j <= sf1; ++j) diag.push_back(a[(j - 1) * sf1 + j - 1 + R.mat[np_].onsite[i]]);
     }
-  return tr;
+  // the sum over the onsite diagonal uses the order-independent exact sum (see orc_exact_sum)
+  double orc_exact_sum(long n, const double* x, const double* y);
+  return orc_exact_sum((long)diag.size(), diag.data(), nullptr);
 }
 
 // matrix_product_trace (mult_module.f90:2885-2916): vdot over storage, sequential sum
@@ -1492,6 +1546,88 @@ double orc_vdot(long n, const double* x, const double* y) {
   double s = 0.0;
   for (long i = 0; i < n; ++i) s += x[i] * y[i];
   return s;
+}
+
+// The reference's vdot/gsum order depends on the BLAS build, so the sum itself
+// is not pinned by the reference.  This is the sum used by the oracle's LNV chain:
+// each term (the rounded product x_i*y_i, or x_i when y is null) is added exactly
+// in fixed point with 150 fraction bits below the largest term's binary
+// exponent (smaller bits truncated toward zero), and the total is rounded once to
+// the nearest double (ties to even).  The result does not depend on term order.
+double orc_exact_sum(long n, const double* x, const double* y) {
+  int emax = INT32_MIN;
+  for (long i = 0; i < n; ++i) {
+    double v = y ? x[i] * y[i] : x[i];
+    if (!std::isfinite(v)) return NAN;
+    if (v != 0.0) { int e; std::frexp(v, &e); if (e > emax) emax = e; }
+  }
+  if (emax == INT32_MIN) return 0.0;
+  const int lsb = emax - 150;
+  // 192-bit two's complement accumulator, limb 0 least significant
+  uint64_t acc[3] = {0, 0, 0};
+  auto add = [&](const uint64_t t[3]) {
+    unsigned __int128 s = (unsigned __int128)acc[0] + t[0];
+    acc[0] = (uint64_t)s;
+    s = (unsigned __int128)acc[1] + t[1] + (uint64_t)(s >> 64);
+    acc[1] = (uint64_t)s;
+    acc[2] = acc[2] + t[2] + (uint64_t)(s >> 64);
+  };
+  for (long i = 0; i < n; ++i) {
+    double v = y ? x[i] * y[i] : x[i];
+    if (v == 0.0) continue;
+    int e;
+    double f = std::frexp(v, &e);
+    long long m = (long long)std::ldexp(f, 53);
+    bool neg = m < 0;
+    unsigned __int128 mag = (unsigned __int128)(neg ? -m : m);
+    int s = e - 53 - lsb;
+    uint64_t t[3] = {0, 0, 0};
+    if (s >= 0) {
+      // place mag << s into the 192-bit word
+      for (int k = 0; k < 3; ++k) {
+        int lo = 64 * k;  // bit range [lo, lo+64) of the word
+        int sh = lo - s;  // word bit b holds mag bit (b - s)
+        uint64_t w = 0;
+        if (sh >= 0) { if (sh < 128) w = (uint64_t)(mag >> sh); }
+        else if (-sh < 64) w = (uint64_t)(mag << (-sh));
+        t[k] = w;
+      }
+    } else if (-s < 64) {
+      t[0] = (uint64_t)(mag >> (-s));
+    }
+    if (neg) {
+      t[0] = ~t[0]; t[1] = ~t[1]; t[2] = ~t[2];
+      uint64_t one[3] = {1, 0, 0};
+      uint64_t tmp[3] = {acc[0], acc[1], acc[2]};
+      acc[0] = t[0]; acc[1] = t[1]; acc[2] = t[2];
+      add(one);
+      t[0] = acc[0]; t[1] = acc[1]; t[2] = acc[2];
+      acc[0] = tmp[0]; acc[1] = tmp[1]; acc[2] = tmp[2];
+    }
+    add(t);
+  }
+  // round to double
+  bool neg = (acc[2] >> 63) != 0;
+  uint64_t w[3] = {acc[0], acc[1], acc[2]};
+  if (neg) {
+    w[0] = ~w[0]; w[1] = ~w[1]; w[2] = ~w[2];
+    if (++w[0] == 0 && ++w[1] == 0) ++w[2];
+  }
+  int h = -1;
+  for (int b = 191; b >= 0; --b)
+    if ((w[b / 64] >> (b % 64)) & 1u) { h = b; break; }
+  if (h < 0) return 0.0;
+  auto bit = [&](int b) -> uint64_t { return b < 0 ? 0 : (w[b / 64] >> (b % 64)) & 1u; };
+  int drop = h > 52 ? h - 52 : 0;
+  uint64_t m = 0;
+  for (int b = h; b >= drop; --b) m = (m << 1) | bit(b);
+  if (drop > 0) {
+    bool half = bit(drop - 1), sticky = false;
+    for (int b = drop - 2; b >= 0; --b) if (bit(b)) { sticky = true; break; }
+    if (half && (sticky || (m & 1))) ++m;
+  }
+  double r = std::ldexp((double)m, lsb + drop);
+  return neg ? -r : r;
 }
 
 }  // extern "C"

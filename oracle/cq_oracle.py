@@ -61,6 +61,8 @@ def _load():
     lib.orc_vdot.restype = c_double
     lib.orc_vdot.argtypes = [c_long, P(c_double), P(c_double)]
     lib.orc_set_dgemm.argtypes = [c_void_p]
+    lib.orc_exact_sum.restype = c_double
+    lib.orc_exact_sum.argtypes = [c_long, P(c_double), P(c_double)]
     # scipy's bundled OpenBLAS provides the dgemm used by the ompGemm kernel (BLAS threads = 1)
     try:
         import scipy
@@ -131,6 +133,24 @@ class OracleSystem:
     def length(self, r):
         return int(self._lib.orc_range_length(self._h, r))
 
+    def blocklist(self, r, coords, cell):
+        """Layout-agnostic description of range r (global atoms, periodic images, radii, offsets)."""
+        from cq_b200.inputs import BlockList
+        nnab = self.geti("n_nab", r)
+        ig_prim = self.geti("ig_prim")
+        ca = self.geti("icover_ibeg")[self.geti("i_part", r) - 1] + self.geti("i_seq", r) - 2   # 0-based cover atom
+        ig_j = self.geti("ig_cover")[ca] - 1
+        xcov = self.getd("xcover").reshape(-1, 3)
+        c = np.asarray(coords, float)
+        xw = c - np.floor((c + 1e-6) / cell) * cell
+        shift = np.rint((xcov[ca] - xw[ig_j]) / cell).astype(np.int64)
+        nd_i = np.repeat(self.geti("ndimi", r), nnab)
+        nd_j = self.geti("ndimj", r)
+        sizes = nd_i * nd_j
+        off = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+        return BlockList(np.repeat(ig_prim, nnab) - 1, ig_j, shift, self.getd("radius", r), nd_i, nd_j, off,
+                         int(sizes.sum()))
+
     # ---- algebra -------------------------------------------------------
     def mat_mult(self, mult_type, ra, rb, rc, a, b, c, kernel="default", nthreads=0):
         """mat_mult(a, b, c) with mat_mult's own roles (multiply_module.f90:115).
@@ -140,7 +160,7 @@ class OracleSystem:
         """
         for arr in (a, b, c):
             assert arr.dtype == np.float64 and arr.flags.c_contiguous
-        k = {"default": 0, "ompGemm": 1}[kernel]
+        k = {"default": 0, "ompGemm": 1, "ompDoii": 2}[kernel]
         st = self._lib.orc_mat_mult(self._h, mult_type, ra, rb, rc, _dp(a), a.size, _dp(b), b.size, _dp(c), c.size,
                                     k, int(nthreads))
         if st != 0:
@@ -158,4 +178,13 @@ class OracleSystem:
         return float(self._lib.orc_matrix_trace(self._h, r, _dp(a)))
 
     def vdot(self, x, y):
+        """Sequential dot product (left to right)."""
         return float(self._lib.orc_vdot(x.size, _dp(x), _dp(y)))
+
+    def exact_dot(self, x, y=None):
+        """Order-independent dot product: exact fixed-point sum of the rounded products, rounded once."""
+        x = np.ascontiguousarray(x, np.float64)
+        if y is None:
+            return float(self._lib.orc_exact_sum(x.size, _dp(x), None))
+        y = np.ascontiguousarray(y, np.float64)
+        return float(self._lib.orc_exact_sum(x.size, _dp(x), _dp(y)))

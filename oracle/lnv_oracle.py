@@ -45,6 +45,132 @@ MULTS = {
 }
 
 
+def bk_inverse(A):
+    """Inverse of a small symmetric matrix by Bunch-Kaufman diagonal pivoting (LAPACK dsytf2 'U',
+    alpha = (1 + sqrt(17)) / 8) and dsytri 'U'.  A is a list of rows (modified copy); returns the
+    full inverse as a list of rows, or None when a pivot block is singular."""
+    n = len(A)
+    a = [row[:] for row in A]          # a[i][j], 0-based
+    alpha = (1.0 + math.sqrt(17.0)) / 8.0
+    ipiv = [0] * n
+    k = n - 1
+    while k >= 0:
+        kstep = 1
+        absakk = abs(a[k][k])
+        imax, colmax = 0, 0.0
+        for i in range(k):
+            if abs(a[i][k]) > colmax:
+                colmax = abs(a[i][k]); imax = i
+        if max(absakk, colmax) == 0.0:
+            return None
+        if absakk >= alpha * colmax:
+            kp = k
+        else:
+            rowmax = 0.0
+            for j in range(imax + 1, k + 1):
+                rowmax = max(rowmax, abs(a[imax][j]))
+            for j in range(imax):
+                rowmax = max(rowmax, abs(a[j][imax]))
+            if absakk >= alpha * colmax * (colmax / rowmax):
+                kp = k
+            elif abs(a[imax][imax]) >= alpha * rowmax:
+                kp = imax
+            else:
+                kp = imax; kstep = 2
+        kk = k - kstep + 1
+        if kp != kk:
+            for i in range(kp):
+                a[i][kk], a[i][kp] = a[i][kp], a[i][kk]
+            for j in range(kp + 1, kk):
+                a[j][kk], a[kp][j] = a[kp][j], a[j][kk]
+            a[kk][kk], a[kp][kp] = a[kp][kp], a[kk][kk]
+            if kstep == 2:
+                a[k - 1][k], a[kp][k] = a[kp][k], a[k - 1][k]
+        if kstep == 1:
+            r1 = 1.0 / a[k][k]
+            for j in range(k - 1, -1, -1):
+                f = -r1 * a[j][k]
+                for i in range(j + 1):
+                    a[i][j] += a[i][k] * f
+            for i in range(k):
+                a[i][k] *= r1
+        elif k > 1:
+            d12 = a[k - 1][k]
+            d22 = a[k - 1][k - 1] / d12
+            d11 = a[k][k] / d12
+            t = 1.0 / (d11 * d22 - 1.0)
+            d12 = t / d12
+            for j in range(k - 2, -1, -1):
+                wkm1 = d12 * (d11 * a[j][k - 1] - a[j][k])
+                wk = d12 * (d22 * a[j][k] - a[j][k - 1])
+                for i in range(j, -1, -1):
+                    a[i][j] = a[i][j] - a[i][k] * wk - a[i][k - 1] * wkm1
+                a[j][k] = wk
+                a[j][k - 1] = wkm1
+        if kstep == 1:
+            ipiv[k] = kp + 1
+        else:
+            ipiv[k] = -(kp + 1); ipiv[k - 1] = -(kp + 1)
+        k -= kstep
+    for i in range(n - 1, -1, -1):
+        if ipiv[i] > 0 and a[i][i] == 0.0:
+            return None
+
+    def inv_col(kc, m):
+        work = [a[i][kc] for i in range(m)]
+        y = []
+        for i in range(m):
+            s = 0.0
+            for j in range(m):
+                s += (a[i][j] if i <= j else a[j][i]) * work[j]
+            y.append(s)
+        for i in range(m):
+            a[i][kc] = -y[i]
+        s = 0.0
+        for i in range(m):
+            s += work[i] * a[i][kc]
+        return s
+
+    k = 0
+    while k < n:
+        if ipiv[k] > 0:
+            a[k][k] = 1.0 / a[k][k]
+            if k > 0:
+                a[k][k] -= inv_col(k, k)
+            kstep = 1
+        else:
+            t = abs(a[k][k + 1])
+            ak = a[k][k] / t
+            akp1 = a[k + 1][k + 1] / t
+            akkp1 = a[k][k + 1] / t
+            d = t * (ak * akp1 - 1.0)
+            a[k][k] = akp1 / d
+            a[k + 1][k + 1] = ak / d
+            a[k][k + 1] = -akkp1 / d
+            if k > 0:
+                a[k][k] -= inv_col(k, k)
+                s = 0.0
+                for i in range(k):
+                    s += a[i][k] * a[i][k + 1]
+                a[k][k + 1] -= s
+                a[k + 1][k + 1] -= inv_col(k + 1, k)
+            kstep = 2
+        kp = abs(ipiv[k]) - 1
+        if kp != k:
+            for i in range(kp):
+                a[i][k], a[i][kp] = a[i][kp], a[i][k]
+            for j in range(kp + 1, k):
+                a[j][k], a[kp][j] = a[kp][j], a[j][k]
+            a[k][k], a[kp][kp] = a[kp][kp], a[k][k]
+            if kstep == 2:
+                a[k][k + 1], a[kp][k + 1] = a[kp][k + 1], a[k][k + 1]
+        k += kstep
+    for i in range(n):
+        for j in range(i + 1, n):
+            a[j][i] = a[i][j]
+    return a
+
+
 class Params:
     def __init__(self, n_L_iterations=50, tolerance=1.0e-7, maxpulay=5, minpulaystep=1.0e-3, maxpulaystep=0.1,
                  lintol=0.1, global_tolerance=False, vary_mu=True, invs_max_steps=100, invs_delta_tol=1.0e-4,
@@ -73,11 +199,12 @@ class Mat:
 class OracleLNV:
     """Density-matrix chain on an OracleSystem whose ranges are named in `ridx` (name -> range index)."""
 
-    def __init__(self, osys, ridx, S, H, ne_spin, n_orbitals, params=None, kernel="default"):
+    def __init__(self, osys, ridx, S, H, ne_spin, n_orbitals, params=None, kernel="ompDoii", nthreads=0):
         self.o = osys
         self.ridx = dict(ridx)
         self.p = params or Params()
         self.kernel = kernel
+        self.nthreads = nthreads
         self.ne = float(ne_spin)            # ne_spin_in_cell(1)
         self.n_o = float(n_orbitals)        # sum of nsf over atoms
         self.ni_in_cell = osys.n_atoms
@@ -104,11 +231,13 @@ class OracleLNV:
         self.n_products += 1
         if t == 1:
             assert A.rng == ra and B.rng == rb and C.rng == rc, mult
-            self.o.mat_mult(1, self.ridx[ra], self.ridx[rb], self.ridx[rc], A.v, B.v, C.v, kernel=self.kernel)
+            self.o.mat_mult(1, self.ridx[ra], self.ridx[rb], self.ridx[rc], A.v, B.v, C.v, kernel=self.kernel,
+                            nthreads=self.nthreads)
         else:
             assert C.rng == ra and B.rng == rb and A.rng == rc, mult
             C.v[:] = 0.0
-            self.o.mat_mult(2, self.ridx[ra], self.ridx[rb], self.ridx[rc], C.v, B.v, A.v, kernel=self.kernel)
+            self.o.mat_mult(2, self.ridx[ra], self.ridx[rb], self.ridx[rc], C.v, B.v, A.v, kernel=self.kernel,
+                            nthreads=self.nthreads)
 
     def msum(self, alpha, A, beta, B):
         """matrix_sum: same range -> scal + axpy, else matrix_add on the shared blocks."""
@@ -125,8 +254,9 @@ class OracleLNV:
         AT.v[:] = self.o.transpose(self.ridx[A.rng], A.v)
 
     def ptrace(self, A, B):
+        """matrix_product_trace: vdot over the storage, summed exactly (order independent)."""
         assert A.rng == B.rng
-        return self.o.vdot(A.v, B.v)
+        return self.o.exact_dot(A.v, B.v)
 
     def trace(self, A):
         return self.o.trace(self.ridx[A.rng], A.v)
@@ -637,19 +767,29 @@ class OracleLNV:
         return p.n_L_iterations, done, deltaE
 
     @staticmethod
-    def do_pulay(iPulay, Aij_in, n, max_n):
-        """DoPulay2D_nospin (Pulay.f90:188-262) with LAPACK dsytrf/dsytri ('U')."""
-        A = np.array(Aij_in[:n, :n], dtype=np.float64, order="F")
+    def do_pulay(iPulay, Aij_in, n, max_n, use_lapack=False):
+        """DoPulay2D_nospin (Pulay.f90:188-262): alphas from the inverse of the residual overlap.
+
+        The inverse follows LAPACK's unblocked Bunch-Kaufman path (dsytrf falls back to dsytf2 for
+        n <= 5, then dsytri, upper triangle) written out below; use_lapack=True calls scipy's LAPACK.
+        """
         invertible = True
         if n == 1:
-            A[0, 0] = 1.0 / A[0, 0]
-        else:
+            A = np.array([[1.0 / Aij_in[0, 0]]])
+        elif use_lapack:
+            A = np.array(Aij_in[:n, :n], dtype=np.float64, order="F")
             lu, ipiv, info = lapack.dsytrf(A, lower=0)
             inv, info2 = lapack.dsytri(lu, ipiv, lower=0)
             if info2 != 0:
                 invertible = False
             else:
                 A = np.triu(inv) + np.triu(inv, 1).T
+        else:
+            A = bk_inverse([[float(Aij_in[i, j]) for j in range(n)] for i in range(n)])
+            if A is None:
+                invertible = False
+            else:
+                A = np.array(A)
         al = np.zeros(max_n)
         if invertible:
             s = 0.0

@@ -42,6 +42,17 @@ def test_cover_dims(cfg2):
     assert np.array_equal(o.geti("cover_dims")[:8], g.geti("cover_dims"))
 
 
+def test_blocklists_identical(cfg2):
+    """The product's layout description equals the oracle's, so generated inputs are identical."""
+    import systems as _s
+    o, g = cfg2
+    coords, cell, _ = _s.config2()
+    for r in range(len(o.rcuts)):
+        a, b = o.blocklist(r, coords, cell), g.blocklist(r, coords, cell)
+        for k in ("ig_i", "ig_j", "shift", "radius", "nd_i", "nd_j", "elem_off"):
+            assert np.array_equal(getattr(a, k), getattr(b, k)), (r, k)
+
+
 @pytest.mark.parametrize("cfg", ["cfg1", "cfg2"])
 def test_range_arrays_bit_exact(cfg, request):
     o, g = request.getfixturevalue(cfg)

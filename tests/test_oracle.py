@@ -102,6 +102,22 @@ def test_type2_and_ompgemm_sz(sz_small):
     assert np.abs(c1 - c2).max() < 1e-12 * np.abs(c1).max()
 
 
+def test_ompdoii_is_bit_identical_to_default(sz_small):
+    coords, cell, o = sz_small
+    blO, blB, blI = [bm.oracle_blocklist(o, r, coords, cell) for r in (1, 2, 3)]
+    a = inputs.random_blocks(blO, 16, 1)
+    b = inputs.random_blocks(blB, 16, 2)
+    c1 = np.zeros(blI.length); c2 = np.zeros(blI.length)
+    o.mat_mult(1, 1, 2, 3, a, b, c1)
+    o.mat_mult(1, 1, 2, 3, a, b, c2, kernel="ompDoii", nthreads=4)
+    assert np.array_equal(c1, c2)
+    cin = inputs.random_blocks(blI, 17, 3)
+    o1 = np.zeros(blO.length); o2 = np.zeros(blO.length)
+    o.mat_mult(2, 1, 2, 3, o1, b, cin)
+    o.mat_mult(2, 1, 2, 3, o2, b, cin, kernel="ompDoii", nthreads=3)
+    assert np.array_equal(o1, o2)
+
+
 def test_transpose_matches_image_arithmetic(sz_small):
     coords, cell, o = sz_small
     for r in range(4):
