@@ -22,6 +22,8 @@ P = ctypes.POINTER
 
 # mirror of the status codes in include/cq_b200.h
 CQ_OK, CQ_ERR_ARG, CQ_ERR_OOM, CQ_ERR_CUDA, CQ_ERR_BOUNDS, CQ_ERR_TIMEOUT, CQ_ERR_STATE, CQ_ERR_NOT_CONVERGED = range(8)
+# product arithmetic (cq_mat_mult precision)
+PREC_FP64_FMA, PREC_FP64, PREC_BF16X3 = 0, 1, 2
 
 
 class LNVParams(ctypes.Structure):
@@ -29,14 +31,15 @@ class LNVParams(ctypes.Structure):
     _fields_ = [("n_L_iterations", c_int), ("tolerance", c_double), ("maxpulay", c_int), ("minpulaystep", c_double),
                 ("maxpulaystep", c_double), ("lintol", c_double), ("global_tolerance", c_int), ("vary_mu", c_int),
                 ("invs_max_steps", c_int), ("invs_delta_tol", c_double), ("invs_tol", c_double), ("exact", c_int),
-                ("max_outer", c_int)]
+                ("max_outer", c_int), ("mixed", c_int), ("mixed_tolerance", c_double)]
 
 
 class LNVResult(ctypes.Structure):
     """cq_lnv_result (include/cq_b200.h)."""
     _fields_ = [("energy", c_double), ("electrons", c_double), ("residual", c_double), ("invs_omega", c_double),
                 ("mcw_sweeps", c_int), ("early_iters", c_int), ("late_iters", c_int), ("ne_corrections", c_int),
-                ("inflexions", c_int), ("converged", c_int), ("n_products", c_int64), ("flops", c_int64)]
+                ("inflexions", c_int), ("converged", c_int), ("n_products", c_int64), ("flops", c_int64),
+                ("n_products_mixed", c_int64), ("flops_mixed", c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -94,6 +97,7 @@ def lib():
         "cq_launch_count": [c_void_p, P(c_int64)],
         "cq_lnv_solve": [c_void_p, P(LNVResult)],
         "cq_pulay_alphas": [c_int, P(c_double), c_int, c_int, P(c_double)],
+        "cq_system_set_option": [c_void_p, c_int, c_int],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -201,13 +205,16 @@ class System:
         return out
 
     # ---- products and algebra on device memory ------------------------------
-    def mat_mult(self, mult_type, ra, rb, rc, a, b, c, exact=True):
-        check(lib().cq_mat_mult(self._h, mult_type, ra, rb, rc, _ptr(a), _ptr(b), _ptr(c), int(bool(exact))))
+    def mat_mult(self, mult_type, ra, rb, rc, a, b, c, exact=True, precision=None):
+        """precision: PREC_FP64 (default kernel rounding), PREC_FP64_FMA, PREC_BF16X3 (tensor cores)."""
+        prec = int(bool(exact)) if precision is None else int(precision)
+        check(lib().cq_mat_mult(self._h, mult_type, ra, rb, rc, _ptr(a), _ptr(b), _ptr(c), prec))
 
-    def mat_mult_host(self, mult_type, ra, rb, rc, a, b, c, exact=True):
+    def mat_mult_host(self, mult_type, ra, rb, rc, a, b, c, exact=True, precision=None):
         for arr in (a, b, c):
             assert arr.dtype == np.float64 and arr.flags.c_contiguous
-        check(lib().cq_mat_mult_host(self._h, mult_type, ra, rb, rc, _dp(a), _dp(b), _dp(c), int(bool(exact))))
+        prec = int(bool(exact)) if precision is None else int(precision)
+        check(lib().cq_mat_mult_host(self._h, mult_type, ra, rb, rc, _dp(a), _dp(b), _dp(c), prec))
 
     def product_work(self, mult_type, ra, rb, rc):
         t, f = c_int64(), c_int64()
@@ -236,6 +243,10 @@ class System:
     def set_stream(self, stream):
         """Enqueue on a cudaStream_t (int handle, e.g. torch.cuda.current_stream().cuda_stream); None = own."""
         check(lib().cq_system_set_stream(self._h, c_void_p(stream) if stream else None))
+
+    def set_mult_variant(self, v):
+        """FP64 4x4 product kernel: 0 = one lane per output element, 1 = one thread per output block."""
+        check(lib().cq_system_set_option(self._h, 1, int(v)))
 
     def profile(self, on=True):
         check(lib().cq_profile_enable(self._h, int(bool(on))))

@@ -145,7 +145,8 @@ int cq_mat_mult(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a
     check_sys(sys); check_range(sys, ra); check_range(sys, rb); check_range(sys, rc);
     CQ_CHECK(a_dev && b_dev && c_dev, CQ_ERR_ARG, "null operand");
     ProductPlan& P = get_plan(sys->S, mult_type, ra, rb, rc);
-    launch_mat_mult(sys->S, P, a_dev, b_dev, c_dev, exact);
+    if (exact == CQ_PREC_BF16X3) mat_mult_mixed(sys->S, mult_type, ra, rb, rc, a_dev, b_dev, c_dev);
+    else launch_mat_mult(sys->S, P, a_dev, b_dev, c_dev, exact);
   });
 }
 
@@ -163,7 +164,8 @@ int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, doub
     if (mult_type == 1) CQ_CUDA(cudaMemcpyAsync(sys->ha.p, a, la * sizeof(double), cudaMemcpyHostToDevice, S.stream));
     CQ_CUDA(cudaMemcpyAsync(sys->hb.p, b, lb * sizeof(double), cudaMemcpyHostToDevice, S.stream));
     if (mult_type == 2) CQ_CUDA(cudaMemcpyAsync(sys->hc.p, c, lc * sizeof(double), cudaMemcpyHostToDevice, S.stream));
-    launch_mat_mult(S, P, sys->ha.p, sys->hb.p, sys->hc.p, exact);
+    if (exact == CQ_PREC_BF16X3) mat_mult_mixed(S, mult_type, ra, rb, rc, sys->ha.p, sys->hb.p, sys->hc.p);
+    else launch_mat_mult(S, P, sys->ha.p, sys->hb.p, sys->hc.p, exact);
     if (mult_type == 1) CQ_CUDA(cudaMemcpyAsync(c, sys->hc.p, lc * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
     else CQ_CUDA(cudaMemcpyAsync(a, sys->ha.p, la * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
     CQ_CUDA(cudaStreamSynchronize(S.stream));
@@ -242,6 +244,18 @@ int cq_profile_read(cq_system* sys, int64_t* launches, double* ms, double* bytes
     if (bytes) *bytes = by;
     if (flops) *flops = fl;
     sys->S.prof.clear();
+  });
+}
+
+int cq_system_set_option(cq_system* sys, int option, int value) {
+  return guarded([&] {
+    check_sys(sys);
+    if (option == CQ_OPT_MULT_VARIANT) {
+      CQ_CHECK(value == 0 || value == 1, CQ_ERR_ARG, "mult variant must be 0 or 1");
+      sys->S.mult_variant = value;
+    } else {
+      throw Error(CQ_ERR_ARG, "unknown option");
+    }
   });
 }
 

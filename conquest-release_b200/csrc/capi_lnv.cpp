@@ -28,6 +28,8 @@ static void fill_result(const LNVStats& st, cq_lnv_result* r) {
   r->converged = st.converged;
   r->n_products = st.n_products;
   r->flops = st.flops;
+  r->n_products_mixed = st.n_products_mixed;
+  r->flops_mixed = st.flops_mixed;
 }
 
 static DMat* matrix_by_name(LNVSolver& L, const char* name) {
@@ -58,6 +60,8 @@ int cq_lnv_params_default(cq_lnv_params* p) {
   p->invs_tol = 1.0e-2;
   p->exact = 1;
   p->max_outer = 1000;
+  p->mixed = 0;
+  p->mixed_tolerance = 1.0e-5;
   return CQ_OK;
 }
 
@@ -149,10 +153,7 @@ int cq_lnv_solve(cq_lnv* s, cq_lnv_result* res) {
   return guarded_call([&] {
     CQ_CHECK(s, CQ_ERR_ARG, "null argument");
     LNVSolver& L = *s->solver;
-    L.stats = LNVStats();
-    L.invert_S();
-    L.delta_e = 0.0;
-    L.find_min_dm(true);
+    L.solve();
     fill_result(L.stats, res);
   });
 }
@@ -163,10 +164,7 @@ int cq_lnv_solve_host(cq_lnv* s, const double* S, const double* H, double* L_out
     LNVSolver& L = *s->solver;
     CQ_CUDA(cudaMemcpyAsync(L.Smat.p, S, sizeof(double) * L.Smat.n, cudaMemcpyHostToDevice, L.S.stream));
     CQ_CUDA(cudaMemcpyAsync(L.Hmat.p, H, sizeof(double) * L.Hmat.n, cudaMemcpyHostToDevice, L.S.stream));
-    L.stats = LNVStats();
-    L.invert_S();
-    L.delta_e = 0.0;
-    L.find_min_dm(true);
+    L.solve();
     if (L_out) CQ_CUDA(cudaMemcpyAsync(L_out, L.L.p, sizeof(double) * L.L.n, cudaMemcpyDeviceToHost, L.S.stream));
     if (K_out) CQ_CUDA(cudaMemcpyAsync(K_out, L.K.p, sizeof(double) * L.K.n, cudaMemcpyDeviceToHost, L.S.stream));
     CQ_CUDA(cudaStreamSynchronize(L.S.stream));

@@ -81,7 +81,40 @@ void LNVSolver::product(const DMat& A, const DMat& B, DMat& C, MultId id) {
 }
 
 void LNVSolver::mult_dispatch(ProductPlan& P, double* a, const double* b, double* c) {
-  launch_mat_mult(S, P, a, b, c, prm.exact);
+  if (use_mixed) {
+    stats.n_products_mixed++;
+    stats.flops_mixed += P.flops;
+    mat_mult_mixed(S, P.mult_type, P.ra, P.rb, P.rc, a, b, c);
+  } else {
+    launch_mat_mult(S, P, a, b, c, prm.exact);
+  }
+}
+
+void LNVSolver::solve() {
+  stats = LNVStats();
+  delta_e = 0.0;
+  if (!prm.mixed) {
+    use_mixed = false;
+    invert_S();
+    find_min_dm(true);
+    return;
+  }
+  // split-precision phase to the hand-over residual, then FP64 from that L to the final tolerance
+  const double tol = prm.tolerance;
+  use_mixed = true;
+  prm.tolerance = prm.mixed_tolerance;
+  try {
+    invert_S();
+    find_min_dm(true);
+  } catch (...) {
+    prm.tolerance = tol;
+    use_mixed = false;
+    throw;
+  }
+  prm.tolerance = tol;
+  use_mixed = false;
+  stats.converged = 0;
+  find_min_dm(false);
 }
 
 void LNVSolver::msum(double alpha, DMat& A, double beta, const DMat& B) {

@@ -33,7 +33,7 @@ struct DMat {
 bool sym_inverse_bk(double* A, int n);
 
 struct LNVStats {
-  int64_t n_products = 0, flops = 0, n_reductions = 0, n_lnv = 0;
+  int64_t n_products = 0, flops = 0, n_reductions = 0, n_lnv = 0, n_products_mixed = 0, flops_mixed = 0;
   int mcw_sweeps = 0, early_iters = 0, late_iters = 0, ne_corrections = 0, inflexions = 0, converged = 0;
   double energy = 0, electrons = 0, last_energy = 0, last_residual = 0, invs_omega = 0;
   double mubar = 0, lambda = 0, hmin = 0, hmax = 0;
@@ -64,6 +64,10 @@ class LNVSolver {
 
   double invert_S();
   void find_min_dm(bool resetL);
+  // complete solve: T = S^-1, FindMinDM from the McWeeny start; with prm.mixed the products run in
+  // split precision until the residual reaches prm.mixed_tolerance, then FindMinDM continues in FP64
+  void solve();
+  bool use_mixed = false;   // current product arithmetic of mult_dispatch
   static void do_pulay(int iPulay, const double* Aij, int n, int max_n, double* al);
   void lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim, double* electrons, double* energy);
 

@@ -179,6 +179,21 @@ struct ProductPlan {
   DevBuf<int2> pairs;             // [n_pairs] (x block, b block)
 };
 
+// Split-precision tensor-core product: pair lists sorted by the first operand block,
+// and groups of consecutive output blocks of one row (one warp each).
+struct MixedPlan {
+  int mult_type = 1, ra = -1, rb = -1, rc = -1, out_range = -1;
+  int n_groups = 0;
+  int64_t n_pairs = 0, flops = 0;
+  DevBuf<int64_t> own_ptr;        // type 2 only (type 1 uses the FP64 plan's lists, already sorted)
+  DevBuf<int2> own_pairs;
+  const int64_t* ptr = nullptr;
+  const int2* pairs = nullptr;
+  DevBuf<int2> groups;
+};
+
+struct FragBuf { DevBuf<uint4> hi, lo; };
+
 struct AddMap {                   // partner of each block of range A in range B (-1 = none)
   DevBuf<int> partner;
 };
@@ -200,6 +215,8 @@ struct System {
   std::vector<std::unique_ptr<RangeIndex>> ranges;
   std::map<std::tuple<int, int, int, int>, std::unique_ptr<ProductPlan>> plans;
   std::map<std::pair<int, int>, std::unique_ptr<AddMap>> addmaps;
+  std::map<std::tuple<int, int, int, int>, std::unique_ptr<MixedPlan>> mplans;
+  std::map<std::pair<int, int>, FragBuf> frags;   // (range, slot) fragment buffers of the mixed products
   cudaStream_t stream = nullptr;
   cudaStream_t own = nullptr;     // the stream created with the system
   bool own_stream = false;
@@ -210,6 +227,7 @@ struct System {
   DevBuf<int> diag_off;           // first onsite-diagonal slot of each primary atom
   DevBuf<double> diag_buf;        // gathered onsite diagonal (exact trace)
   int64_t launches = 0;           // kernels launched by this system (all kinds)
+  int mult_variant = 1;           // 4x4 FP64 product kernel: 0 = one lane per element, 1 = one thread per block
   ProductProfile prof;
   ~System();
 };
@@ -221,8 +239,17 @@ ProductPlan& get_plan(System& S, int mult_type, int ra, int rb, int rc);
 AddMap& get_addmap(System& S, int ra, int rb);
 void export_range_array(System& S, int r, const std::string& name, std::vector<int64_t>& out);
 
+MixedPlan& get_mixed_plan(System& S, int mult_type, int ra, int rb, int rc);
+
 // mult.cu
 void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, double* c, int exact);
+
+// mixed.cu
+void to_fragments(System& S, int r, const double* src, int role_b, int trans, uint4* hi, uint4* lo);
+void launch_mult_tc(System& S, MixedPlan& MP, const uint4* xa_hi, const uint4* xa_lo, const uint4* bb_hi,
+                    const uint4* bb_lo, double* out);
+// split-precision mat_mult with the roles of launch_mat_mult (fragments converted per call)
+void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c);
 
 // algebra.cu
 void dev_scale(System& S, double* a, int64_t n, double alpha);

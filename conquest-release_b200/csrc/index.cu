@@ -300,6 +300,44 @@ __global__ void k_plan2(PlanArgs A, int nnz_out, int pass, int* __restrict__ cnt
   }
 }
 
+// type 2, lists ordered by the input block: one warp per output block (p, k); lanes walk row p of
+// the input c, map each neighbour j back into the frame of k's home atom and look it up in B's row.
+// Label of j in kh's frame = label(j in p's frame) - label(k's partition) + label(kh's home partition).
+__global__ void k_plan2x(PlanArgs A, int nnz_out, int pass, const int* __restrict__ prim_cover_label, int ncx, int ncy,
+                         int ncz, int* __restrict__ cnt, const int64_t* __restrict__ ptr, int2* __restrict__ pairs) {
+  int warp = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp, lane = threadIdx.x % kWarp;
+  if (warp >= nnz_out) return;
+  const int eo = warp;
+  const int p = A.a_row[eo];
+  const int k = A.a_cover[eo];
+  const int kh = A.cover_home_prim[k];
+  const int yz = ncy * ncz;
+  auto xyz = [&](int lab, int& x, int& y, int& z) { int l = lab - 1; x = l / yz; y = (l - x * yz) / ncz; z = l - x * yz - y * ncz; };
+  int kx, ky, kz, hx, hy, hz;
+  xyz(A.cover_label_of_part[A.cover_part[k]], kx, ky, kz);
+  xyz(prim_cover_label[kh], hx, hy, hz);
+  const unsigned lt = (1u << lane) - 1u;
+  int n = 0;
+  int64_t base = pass ? ptr[eo] : 0;
+  for (int ex0 = A.c_row_ptr[p]; ex0 < A.c_row_ptr[p + 1]; ex0 += kWarp) {
+    int ex = ex0 + lane, eb = -1;
+    if (ex < A.c_row_ptr[p + 1]) {
+      int c = A.c_cover[ex];
+      int cx, cy, cz;
+      xyz(A.cover_label_of_part[A.cover_part[c]], cx, cy, cz);
+      int tx = cx - kx + hx, ty = cy - ky + hy, tz = cz - kz + hz;
+      if (tx >= 0 && tx < ncx && ty >= 0 && ty < ncy && tz >= 0 && tz < ncz) {
+        int np_ = A.label_to_cover[tx * yz + ty * ncz + tz + 1];
+        if (np_ >= 0) eb = find_in_row(A.b_row_ptr, A.b_cover, kh, A.cover_first[np_] + A.cover_seq[c] - 1);
+      }
+    }
+    unsigned m = __ballot_sync(0xffffffffu, eb >= 0);
+    if (pass == 1 && eb >= 0) pairs[base + n + __popc(m & lt)] = make_int2(ex, eb);
+    n += __popc(m);
+  }
+  if (pass == 0 && lane == 0) cnt[eo] = n;
+}
+
 // partner block of each block of range A in range B (same row, same cover atom), or -1
 __global__ void k_addmap(int nnz, const int* __restrict__ a_row, const int* __restrict__ a_cover,
                          const int* __restrict__ b_row_ptr, const int* __restrict__ b_cover, int* __restrict__ partner) {
@@ -553,6 +591,60 @@ ProductPlan& get_plan(System& S, int mult_type, int ra, int rb, int rc) {
   CQ_CUDA(cudaGetLastError());
   CQ_CHECK(read_flag(err.p, st) == 0, CQ_ERR_BOUNDS, "pair list: lookup failed");
   auto res = S.plans.emplace(key, std::move(plan));
+  return *res.first->second;
+}
+
+MixedPlan& get_mixed_plan(System& S, int mult_type, int ra, int rb, int rc) {
+  auto key = std::make_tuple(mult_type, ra, rb, rc);
+  auto it = S.mplans.find(key);
+  if (it != S.mplans.end()) return *it->second;
+  ProductPlan& P = get_plan(S, mult_type, ra, rb, rc);
+  auto mp = std::make_unique<MixedPlan>();
+  MixedPlan& M = *mp;
+  M.mult_type = mult_type; M.ra = ra; M.rb = rb; M.rc = rc;
+  M.out_range = P.out_range;
+  M.flops = P.flops;
+  M.n_pairs = P.n_pairs;
+  cudaStream_t st = S.stream;
+  if (mult_type == 1) {
+    // type-1 lists follow row i of A in order: already sorted by the first operand
+    M.ptr = P.ptr.p;
+    M.pairs = P.pairs.p;
+  } else {
+    RangeIndex &A = *S.ranges[ra], &B = *S.ranges[rb], &C = *S.ranges[rc];
+    DevGeometry& d = S.dg;
+    PlanArgs pa;
+    pa.a_row_ptr = A.row_ptr.p; pa.a_cover = A.nb_cover.p; pa.a_row = A.nb_row.p;
+    pa.b_row_ptr = B.row_ptr.p; pa.b_cover = B.nb_cover.p; pa.b_ibpart = B.nb_ibpart.p;
+    pa.c_row_ptr = C.row_ptr.p; pa.c_cover = C.nb_cover.p;
+    pa.cover_part = d.cover_part.p; pa.cover_label_of_part = d.cover_label_of_part.p;
+    pa.cover_home_prim = d.cover_home_prim.p; pa.label_to_cover = d.label_to_cover.p; pa.cover_first = d.cover_first.p;
+    pa.cover_seq = d.cover_seq.p; pa.cover_nsf = d.cover_nsf.p; pa.prim_nsf = d.prim_nsf.p;
+    pa.ng_cover = S.geo.ng_cover;
+    const int nout = A.nnz, T = 256, WPB = T / kWarp;
+    DevBuf<int> cnt;
+    cnt.alloc(std::max(nout, 1));
+    const int* g = S.geo.ncover;
+    if (nout) k_plan2x<<<nblk(nout, WPB), T, 0, st>>>(pa, nout, 0, d.prim_cover_label.p, g[0], g[1], g[2], cnt.p, nullptr, nullptr);
+    CQ_CUDA(cudaGetLastError());
+    M.own_ptr.alloc(nout + 1);
+    int64_t np2 = exclusive_scan(cnt.p, nout, M.own_ptr.p, st);
+    CQ_CHECK(np2 == P.n_pairs, CQ_ERR_STATE, "type-2 lists by input block disagree with the default-order lists");
+    M.own_pairs.alloc(std::max<int64_t>(np2, 1));
+    if (nout) k_plan2x<<<nblk(nout, WPB), T, 0, st>>>(pa, nout, 1, d.prim_cover_label.p, g[0], g[1], g[2], nullptr, M.own_ptr.p, M.own_pairs.p);
+    CQ_CUDA(cudaGetLastError());
+    M.ptr = M.own_ptr.p;
+    M.pairs = M.own_pairs.p;
+  }
+  // groups of up to 8 consecutive output blocks of one row
+  RangeIndex& O = *S.ranges[M.out_range];
+  std::vector<int2> grp;
+  for (int p = 0; p < S.geo.n_prim; ++p)
+    for (int s = O.h_row_ptr[p]; s < O.h_row_ptr[p + 1]; s += 8) grp.push_back(make_int2(s, std::min(8, O.h_row_ptr[p + 1] - s)));
+  M.n_groups = (int)grp.size();
+  M.groups.upload(grp, st);
+  CQ_CUDA(cudaStreamSynchronize(st));
+  auto res = S.mplans.emplace(key, std::move(mp));
   return *res.first->second;
 }
 

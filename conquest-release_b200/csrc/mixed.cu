@@ -1,0 +1,216 @@
+// Split-precision block products on the tensor cores (blocks of up to 16 x 16).
+//
+// Each FP64 operand block is padded to 16 x 16 and split into two bf16 parts,
+// v = hi + lo (hi = bf16(v), lo = bf16(v - hi)); a block product is the sum of
+// hi.hi + hi.lo + lo.hi (three bf16 MMAs, FP32 accumulation), which carries
+// about 16 significant bits per term.  The result is written back as FP64 into
+// the block storage of the output range, so the matrices of the chain stay FP64.
+//
+// Work decomposition (output stationary, same pair lists as the FP64 path):
+// one warp owns G consecutive output blocks of one output row i.  Their pair
+// lists are sorted by the first operand block (A_ik for type 1, C_ij for type 2,
+// both in row i), so the warp walks the union of those blocks in order, loads each
+// first-operand fragment once and multiplies it into every output block whose list
+// contains it.  Operands are pre-converted into the per-lane fragment order of
+// mma.m16n8k16, so every fragment is one coalesced 16-byte load per lane.
+#include <cuda_bf16.h>
+
+#include <climits>
+
+#include "cq_internal.hpp"
+
+namespace cqb {
+namespace {
+
+constexpr int kG = 8;   // output blocks per warp
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo_k, __nv_bfloat16 hi_k) {
+  return (uint32_t)__bfloat16_as_ushort(lo_k) | ((uint32_t)__bfloat16_as_ushort(hi_k) << 16);
+}
+
+// element (r, c) of a padded 16 x 16 view of a column-major nd_r x nd_c FP64 block
+__device__ __forceinline__ double blk_at(const double* B, int nd_r, int nd_c, int r, int c) {
+  return (r < nd_r && c < nd_c) ? B[r + nd_r * c] : 0.0;
+}
+
+__device__ __forceinline__ void split2(double v, __nv_bfloat16& h, __nv_bfloat16& l) {
+  h = __double2bfloat16(v);
+  l = __double2bfloat16(v - (double)__bfloat162float(h));
+}
+
+// A-role fragments (M = block rows, K = block columns):
+//   reg0 (row g,   k 2t..2t+1), reg1 (row g+8, k 2t..2t+1), reg2 (row g, k 2t+8..), reg3 (row g+8, k 2t+8..)
+// B-role fragments (K = block rows, N = block columns; `trans` uses the transposed block),
+//   two n8 tiles: {tile0 (k 2t.., n g), tile0 (k 2t+8.., n g), tile1 (k 2t.., n g+8), tile1 (k 2t+8.., n g+8)}
+__global__ void k_to_frag(int nnz, const int64_t* __restrict__ elem, const int* __restrict__ row,
+                          const int* __restrict__ cover, const int* __restrict__ prim_nsf,
+                          const int* __restrict__ cover_nsf, const double* __restrict__ src, int role_b, int trans,
+                          uint4* __restrict__ hi, uint4* __restrict__ lo) {
+  int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int e = (int)(tid >> 5), lane = (int)(tid & 31);
+  if (e >= nnz) return;
+  const int ndr = prim_nsf[row[e]], ndc = cover_nsf[cover[e]];
+  const double* B = src + elem[e];
+  const int g = lane >> 2, t = lane & 3;
+  int rr[8], cc[8];
+  if (!role_b) {
+    const int r0[4] = {g, g + 8, g, g + 8}, c0[4] = {2 * t, 2 * t, 2 * t + 8, 2 * t + 8};
+    for (int q = 0; q < 4; ++q) { rr[2 * q] = r0[q]; cc[2 * q] = c0[q]; rr[2 * q + 1] = r0[q]; cc[2 * q + 1] = c0[q] + 1; }
+  } else {
+    // (K, N) pairs; element (K=k, N=n) is block (k, n), or block (n, k) when transposed
+    const int k0[4] = {2 * t, 2 * t + 8, 2 * t, 2 * t + 8}, n0[4] = {g, g, g + 8, g + 8};
+    for (int q = 0; q < 4; ++q) {
+      for (int h = 0; h < 2; ++h) {
+        int k = k0[q] + h, n = n0[q];
+        rr[2 * q + h] = trans ? n : k;
+        cc[2 * q + h] = trans ? k : n;
+      }
+    }
+  }
+  uint32_t wh[4], wl[4];
+  for (int q = 0; q < 4; ++q) {
+    __nv_bfloat16 h0, l0, h1, l1;
+    split2(blk_at(B, ndr, ndc, rr[2 * q], cc[2 * q]), h0, l0);
+    split2(blk_at(B, ndr, ndc, rr[2 * q + 1], cc[2 * q + 1]), h1, l1);
+    wh[q] = pack_bf16(h0, h1);
+    wl[q] = pack_bf16(l0, l1);
+  }
+  hi[(int64_t)e * 32 + lane] = make_uint4(wh[0], wh[1], wh[2], wh[3]);
+  lo[(int64_t)e * 32 + lane] = make_uint4(wl[0], wl[1], wl[2], wl[3]);
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint4& a, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a.x), "r"(a.y), "r"(a.z), "r"(a.w), "r"(b0), "r"(b1));
+}
+
+struct TCArgs {
+  const int2* __restrict__ groups;     // (first output block, count) per warp, never crossing a row
+  int n_groups;
+  const int64_t* __restrict__ ptr;     // pair list offsets per output block
+  const int2* __restrict__ pairs;      // (first-operand block, B block), first operand ascending
+  const uint4* __restrict__ xa_hi;     // first operand, A-role fragments
+  const uint4* __restrict__ xa_lo;
+  const uint4* __restrict__ bb_hi;     // B operand, B-role fragments
+  const uint4* __restrict__ bb_lo;
+  const int* __restrict__ o_row;
+  const int* __restrict__ o_cover;
+  const int64_t* __restrict__ o_elem;
+  const int* __restrict__ prim_nsf;
+  const int* __restrict__ cover_nsf;
+  double* __restrict__ out;
+};
+
+__global__ void __launch_bounds__(128) k_mult_tc(TCArgs M) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= M.n_groups) return;
+  const int2 grp = M.groups[w];
+  int64_t p[kG], pe[kG];
+  int nx[kG];
+  float acc[kG][2][4];
+#pragma unroll
+  for (int b = 0; b < kG; ++b) {
+    if (b < grp.y) { p[b] = M.ptr[grp.x + b]; pe[b] = M.ptr[grp.x + b + 1]; }
+    else { p[b] = 0; pe[b] = 0; }
+    nx[b] = p[b] < pe[b] ? M.pairs[p[b]].x : INT_MAX;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[b][h][r] = 0.f;
+  }
+  while (true) {
+    int kc = INT_MAX;
+#pragma unroll
+    for (int b = 0; b < kG; ++b) kc = min(kc, nx[b]);
+    if (kc == INT_MAX) break;
+    const uint4 ah = __ldg(M.xa_hi + (int64_t)kc * 32 + lane);
+    const uint4 al = __ldg(M.xa_lo + (int64_t)kc * 32 + lane);
+#pragma unroll
+    for (int b = 0; b < kG; ++b) {
+      if (nx[b] == kc) {
+        const int y = M.pairs[p[b]].y;
+        const uint4 bh = __ldg(M.bb_hi + (int64_t)y * 32 + lane);
+        const uint4 bl = __ldg(M.bb_lo + (int64_t)y * 32 + lane);
+        mma_bf16(acc[b][0], al, bh.x, bh.y);
+        mma_bf16(acc[b][0], ah, bl.x, bl.y);
+        mma_bf16(acc[b][0], ah, bh.x, bh.y);
+        mma_bf16(acc[b][1], al, bh.z, bh.w);
+        mma_bf16(acc[b][1], ah, bl.z, bl.w);
+        mma_bf16(acc[b][1], ah, bh.z, bh.w);
+        ++p[b];
+        nx[b] = p[b] < pe[b] ? M.pairs[p[b]].x : INT_MAX;
+      }
+    }
+  }
+  const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+  for (int b = 0; b < kG; ++b) {
+    if (b < grp.y) {
+      const int q = grp.x + b;
+      const int ndr = M.prim_nsf[M.o_row[q]], ndc = M.cover_nsf[M.o_cover[q]];
+      double* O = M.out + M.o_elem[q];
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          int row = g + ((r & 2) ? 8 : 0), col = 8 * h + 2 * t + (r & 1);
+          if (row < ndr && col < ndc) O[row + ndr * col] = (double)acc[b][h][r];
+        }
+    }
+  }
+}
+
+}  // namespace
+
+// A-role (first operand) or B-role fragments of a whole range, hi and lo parts (1 KB per block)
+void to_fragments(System& S, int r, const double* src, int role_b, int trans, uint4* hi, uint4* lo) {
+  RangeIndex& R = *S.ranges[r];
+  if (R.nnz == 0) return;
+  int64_t threads = (int64_t)R.nnz * 32;
+  k_to_frag<<<(int)((threads + 255) / 256), 256, 0, S.stream>>>(R.nnz, R.nb_elem.p, R.nb_row.p, R.nb_cover.p,
+                                                                S.dg.prim_nsf.p, S.dg.cover_nsf.p, src, role_b, trans,
+                                                                hi, lo);
+  S.launches++;
+  CQ_CUDA(cudaGetLastError());
+}
+
+static FragBuf& frag_buffer(System& S, int r, int slot) {
+  FragBuf& f = S.frags[std::make_pair(r, slot)];
+  size_t need = (size_t)std::max(S.ranges[r]->nnz, 1) * 32;
+  if (f.hi.n < need) { f.hi.alloc(need); f.lo.alloc(need); }
+  return f;
+}
+
+void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c) {
+  MixedPlan& MP = get_mixed_plan(S, mult_type, ra, rb, rc);
+  int rx = mult_type == 1 ? ra : rc;
+  const double* x = mult_type == 1 ? a : c;
+  double* out = mult_type == 1 ? c : a;
+  FragBuf& fx = frag_buffer(S, rx, 0);
+  FragBuf& fb = frag_buffer(S, rb, 1);
+  to_fragments(S, rx, x, 0, 0, fx.hi.p, fx.lo.p);
+  to_fragments(S, rb, b, 1, mult_type == 2 ? 1 : 0, fb.hi.p, fb.lo.p);
+  launch_mult_tc(S, MP, fx.hi.p, fx.lo.p, fb.hi.p, fb.lo.p, out);
+}
+
+void launch_mult_tc(System& S, MixedPlan& MP, const uint4* xa_hi, const uint4* xa_lo, const uint4* bb_hi,
+                    const uint4* bb_lo, double* out) {
+  RangeIndex& O = *S.ranges[MP.out_range];
+  TCArgs M;
+  M.groups = MP.groups.p;
+  M.n_groups = MP.n_groups;
+  M.ptr = MP.ptr;
+  M.pairs = MP.pairs;
+  M.xa_hi = xa_hi; M.xa_lo = xa_lo; M.bb_hi = bb_hi; M.bb_lo = bb_lo;
+  M.o_row = O.nb_row.p; M.o_cover = O.nb_cover.p; M.o_elem = O.nb_elem.p;
+  M.prim_nsf = S.dg.prim_nsf.p; M.cover_nsf = S.dg.cover_nsf.p;
+  M.out = out;
+  if (MP.n_groups == 0) return;
+  k_mult_tc<<<(MP.n_groups * 32 + 127) / 128, 128, 0, S.stream>>>(M);
+  S.launches++;
+  CQ_CUDA(cudaGetLastError());
+}
+
+}  // namespace cqb

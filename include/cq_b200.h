@@ -91,18 +91,25 @@ int cq_export_radius(cq_system* sys, int r, double* out, int64_t cap, int64_t* n
  * src/multiply_kernel_default.f90:132-224, 325-412).
  *   mult_type 1: c_dev (range rc) = a_dev (range ra) . b_dev (range rb)
  *   mult_type 2: a_dev (range ra) = c_dev (range rc) . b_dev^T (range rb)
- * exact != 0 keeps the reference's separate multiply and add per term
- * (bit-identical to the default kernel built without FMA contraction);
- * exact == 0 fuses them.  The pair lists of the product are built on the
- * first call and cached.  Work is enqueued on the system's stream; the call
- * returns without synchronising.
+ * `precision` selects the arithmetic:
+ *   CQ_PREC_FP64 (1): FP64 with the reference's separate multiply and add per
+ *     term, bit-identical to the default kernel built without FMA contraction;
+ *   CQ_PREC_FP64_FMA (0): FP64 with fused multiply-add;
+ *   CQ_PREC_BF16X3 (2): blocks padded to 16 x 16 and split v = hi + lo in bf16,
+ *     hi.hi + hi.lo + lo.hi on the tensor cores with FP32 accumulation, stored
+ *     back as FP64 (about 16 significant bits per product term).
+ * The pair lists of the product are built on the first call and cached.  Work
+ * is enqueued on the system's stream; the call returns without synchronising.
  */
+#define CQ_PREC_FP64_FMA 0
+#define CQ_PREC_FP64 1
+#define CQ_PREC_BF16X3 2
 int cq_mat_mult(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a_dev, const double* b_dev,
-                double* c_dev, int exact);
+                double* c_dev, int precision);
 
 /* Same as cq_mat_mult with host arrays: copies in, multiplies, copies the result out, synchronises. */
 int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c,
-                     int exact);
+                     int precision);
 
 /* Algorithmic work of one product: (k,i,j) triples with a stored result and 2*sum nd^3 flops. */
 int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* triples, int64_t* flops);
@@ -155,6 +162,11 @@ int cq_profile_read(cq_system* sys, int64_t* launches, double* ms, double* bytes
 /* Kernels launched by this system so far (all kinds). */
 int cq_launch_count(cq_system* sys, int64_t* count);
 
+/* Tuning options.  CQ_OPT_MULT_VARIANT: FP64 4x4 product kernel, 0 = one lane per output
+ * element, 1 = one thread per output block (default).  Both give identical results. */
+#define CQ_OPT_MULT_VARIANT 1
+int cq_system_set_option(cq_system* sys, int option, int value);
+
 /* ------------------------------------------------------------------------ */
 /* LNV / McWeeny density-matrix minimisation (one spin channel, nspin = 1)   */
 /* ------------------------------------------------------------------------ */
@@ -176,6 +188,9 @@ typedef struct {
   double invs_tol;         /* DM.InvSTolerance (1e-2) */
   int exact;               /* 1: FP64 products with the default kernel's rounding; 0: fused multiply-add */
   int max_outer;           /* bound on FindMinDM outer iterations (the reference loops until done) */
+  int mixed;               /* 1: cq_lnv_solve runs Hotelling and FindMinDM with CQ_PREC_BF16X3 products, then
+                              continues FindMinDM from that L with FP64 products to `tolerance` */
+  double mixed_tolerance;  /* residual at which the split-precision phase hands over to FP64 */
 } cq_lnv_params;
 
 typedef struct {
@@ -186,6 +201,8 @@ typedef struct {
   int mcw_sweeps, early_iters, late_iters, ne_corrections, inflexions, converged;
   int64_t n_products;      /* block-sparse products executed */
   int64_t flops;           /* algorithmic flops of those products (2 sum nd_i nd_j nd_k) */
+  int64_t n_products_mixed;/* of which with split-precision tensor-core arithmetic */
+  int64_t flops_mixed;
 } cq_lnv_result;
 
 int cq_lnv_params_default(cq_lnv_params* p);

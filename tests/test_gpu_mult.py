@@ -71,6 +71,27 @@ def test_type1_dzp_bit_exact(cfg1):
     assert f == 2 * 13 ** 3 * t and t > 0
 
 
+@pytest.mark.parametrize("mult_type", [1, 2])
+def test_bf16x3_tensor_core_products(cfg1, mult_type):
+    """Split-precision products: per element within 2^-14 of sum |a||b| (about 16 bits per term)."""
+    import cq_b200
+    o, g, bls = cfg1
+    b = inputs.random_blocks(bls[1], 13, inputs.TAG_RANDOM_B)
+    if mult_type == 1:
+        a = inputs.random_blocks(bls[0], 13, inputs.TAG_RANDOM_A)
+        ref = np.zeros(bls[2].length); o.mat_mult(1, 0, 1, 2, a, b, ref)
+        got = np.zeros(bls[2].length); g.mat_mult_host(1, 0, 1, 2, a, b, got, precision=cq_b200.PREC_BF16X3)
+        bound = _abs_bound(o, 1, 0, 1, 2, a, b, ref)
+    else:
+        cin = inputs.random_blocks(bls[2], 14, inputs.TAG_RANDOM_A)
+        ref = np.zeros(bls[0].length); o.mat_mult(2, 0, 1, 2, ref, b, cin)
+        got = np.zeros(bls[0].length); g.mat_mult_host(2, 0, 1, 2, got, b, cin, precision=cq_b200.PREC_BF16X3)
+        bound = _abs_bound(o, 2, 0, 1, 2, ref, b, cin)
+    err = np.abs(got - ref)
+    assert np.all(err <= 2.0 ** -14 * bound + 1e-300)
+    assert err.max() > 0          # it really ran in reduced precision
+
+
 def test_type2_dzp_bit_exact(cfg1):
     o, g, bls = cfg1
     b = inputs.random_blocks(bls[1], 12, inputs.TAG_RANDOM_B)
@@ -89,9 +110,11 @@ LNV_PRODUCTS = [  # (type, a range, b range, c range) in mat_mult roles, from th
 ]
 
 
+@pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("prod", LNV_PRODUCTS)
-def test_lnv_products_sz_bit_exact(cfg2, prod):
+def test_lnv_products_sz_bit_exact(cfg2, prod, variant):
     o, g, bls, idx = cfg2
+    g.set_mult_variant(variant)
     t, ra, rb, rc = prod
     ia, ib, ic = idx[ra], idx[rb], idx[rc]
     a = inputs.random_blocks(bls[ra], 21, inputs.TAG_RANDOM_A)
