@@ -98,6 +98,7 @@ def lib():
         "cq_lnv_solve": [c_void_p, P(LNVResult)],
         "cq_pulay_alphas": [c_int, P(c_double), c_int, c_int, P(c_double)],
         "cq_system_set_option": [c_void_p, c_int, c_int],
+        "cq_generate_SH": [c_void_p, c_int, c_int, ctypes.c_uint64, c_void_p],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -261,6 +262,14 @@ class System:
         check(lib().cq_launch_count(self._h, ctypes.byref(n)))
         return n.value
 
+    def generate_SH(self, r, which, seed, out):
+        """Synthetic S (which=0) or H (which=1) of range r into the device array `out`, stream-ordered."""
+        check(lib().cq_generate_SH(self._h, int(r), int(which), int(seed), _ptr(out)))
+
+    def set_blocking_sync(self, on=True):
+        """Host waits for device scalars sleep on a blocking-sync event (many solvers per core)."""
+        check(lib().cq_system_set_option(self._h, 2, int(bool(on))))
+
     def blocklist(self, r, coords, cell):
         """Layout-agnostic description of range r (global atoms, images, radii, offsets) for the input generators."""
         from .inputs import BlockList
@@ -377,3 +386,119 @@ def pulay_alphas(ipulay, Aij, n, max_n):
     al = np.zeros(max_n)
     check(lib().cq_pulay_alphas(int(ipulay), Af.ctypes.data_as(P(c_double)), int(n), int(max_n), _dp(al)))
     return al
+
+
+# --------------------------------------------------------------------------
+# serving loop (cq_server_*): continuous batching of independent solves
+# --------------------------------------------------------------------------
+class ServerConfig(ctypes.Structure):
+    """cq_server_config (include/cq_b200.h)."""
+    _fields_ = [("n_slots", c_int), ("hbm_budget", c_int64), ("max_bypass", c_int), ("blocking_sync", c_int),
+                ("dry_run", c_int), ("dry_run_seconds", c_double), ("lnv", LNVParams)]
+
+
+class Request(ctypes.Structure):
+    """cq_request (include/cq_b200.h)."""
+    _fields_ = [("n_atoms", c_int), ("coords", P(c_double)), ("cell", P(c_double)), ("nsf", P(c_int)),
+                ("rs", c_double), ("rh", c_double), ("rl", c_double), ("rt", c_double), ("ne_spin", c_double),
+                ("seed", ctypes.c_uint64), ("mixed", c_int), ("t_arrival", c_double)]
+
+
+class RequestResult(ctypes.Structure):
+    """cq_request_result (include/cq_b200.h)."""
+    _fields_ = [("id", c_int64), ("status", c_int), ("n_atoms", c_int), ("converged", c_int), ("mixed", c_int),
+                ("slot", c_int), ("energy", c_double), ("electrons", c_double), ("residual", c_double),
+                ("n_products", c_int64), ("flops", c_int64), ("n_products_mixed", c_int64), ("flops_mixed", c_int64),
+                ("t_arrival", c_double), ("t_admit", c_double), ("t_done", c_double), ("bytes_estimate", c_int64),
+                ("bytes_peak", c_int64), ("message", ctypes.c_char * 128)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["message"] = self.message.decode(errors="replace")
+        d["latency"] = self.t_done - self.t_arrival
+        return d
+
+
+def _server_lib():
+    L = lib()
+    if not getattr(L, "_server_sigs", False):
+        sigs = {
+            "cq_server_config_default": [P(ServerConfig)],
+            "cq_server_create": [P(ServerConfig), P(c_void_p)],
+            "cq_server_submit": [c_void_p, P(Request), P(c_int64)],
+            "cq_server_wait": [c_void_p, c_int64, c_double, P(RequestResult)],
+            "cq_server_now": [c_void_p, P(c_double)],
+            "cq_request_estimate": [P(Request), P(c_int64)],
+            "cq_server_destroy": [c_void_p],
+        }
+        for name, args in sigs.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = c_int
+        L._server_sigs = True
+    return L
+
+
+def _request(coords, cell, nsf, rs, rh, rl, rt, ne_spin, seed=0, mixed=False, t_arrival=-1.0):
+    coords = np.ascontiguousarray(coords, np.float64).reshape(-1, 3)
+    cell = np.ascontiguousarray(cell, np.float64)
+    nsf = np.ascontiguousarray(np.broadcast_to(nsf, (len(coords),)), np.int32)
+    r = Request(len(coords), _dp(coords), _dp(cell), _ip(nsf), rs, rh, rl, rt, float(ne_spin), int(seed),
+                int(bool(mixed)), float(t_arrival))
+    return r, (coords, cell, nsf)   # the arrays must stay alive while the request is read
+
+
+def request_estimate(coords, cell, nsf, rs, rh, rl, rt, ne_spin=1.0, mixed=False):
+    """Device bytes the server's admission reserves for this solve."""
+    r, keep = _request(coords, cell, nsf, rs, rh, rl, rt, ne_spin, mixed=mixed)
+    b = c_int64()
+    check(_server_lib().cq_request_estimate(ctypes.byref(r), ctypes.byref(b)))
+    return b.value
+
+
+class Server:
+    """Continuous-batching server of density-matrix solves (cq_server_*).
+
+    Each request is one system given by its geometry and ranges; S and H are generated on the
+    device from `seed`, and the result carries energy, electron count, work and latency.
+    """
+
+    def __init__(self, n_slots=8, hbm_budget=64 << 30, max_bypass=4, blocking_sync=True, dry_run=False,
+                 dry_run_seconds=0.01, **lnv):
+        L = _server_lib()
+        c = ServerConfig()
+        check(L.cq_server_config_default(ctypes.byref(c)))
+        c.n_slots, c.hbm_budget, c.max_bypass = int(n_slots), int(hbm_budget), int(max_bypass)
+        c.blocking_sync, c.dry_run, c.dry_run_seconds = int(bool(blocking_sync)), int(bool(dry_run)), float(dry_run_seconds)
+        for k, v in lnv.items():
+            setattr(c.lnv, k, v)
+        h = c_void_p()
+        check(L.cq_server_create(ctypes.byref(c), ctypes.byref(h)))
+        self._h = h
+
+    def submit(self, coords, cell, nsf, rs, rh, rl, rt, ne_spin, seed=0, mixed=False, t_arrival=-1.0):
+        r, keep = _request(coords, cell, nsf, rs, rh, rl, rt, ne_spin, seed, mixed, t_arrival)
+        i = c_int64()
+        check(_server_lib().cq_server_submit(self._h, ctypes.byref(r), ctypes.byref(i)))
+        return i.value
+
+    def wait(self, rid, timeout=-1.0):
+        out = RequestResult()
+        check(_server_lib().cq_server_wait(self._h, int(rid), float(timeout), ctypes.byref(out)))
+        return out.as_dict()
+
+    def now(self):
+        t = c_double()
+        check(_server_lib().cq_server_now(self._h, ctypes.byref(t)))
+        return t.value
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _server_lib().cq_server_destroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -72,6 +72,7 @@ __global__ void k_transpose(int nnz, const int* __restrict__ dest, const int64_t
 // Terms below 2^(emax-150) are truncated toward zero (relative effect < n 2^-150).
 // ---------------------------------------------------------------------------
 constexpr int kAccFrac = 150;   // fraction bits kept below the largest term's exponent
+constexpr int kEBias = 2048;    // exponent bias of the pass-1 maximum (frexp exponents lie in [-1073, 1024])
 
 struct Acc192 { uint64_t w[3]; };
 
@@ -111,18 +112,19 @@ __device__ __forceinline__ void acc_term(Acc192& a, double v, int lsb_exp) {
 __device__ __forceinline__ double dterm(const double* x, const double* y, int64_t i) {
   return y ? __dmul_rn(x[i], y[i]) : x[i];
 }
-// pass 1: largest exponent of the nonzero terms; a non-finite term sets the flag
+// pass 1: largest exponent of the nonzero terms, stored biased by kEBias (0 = every term is zero);
+// a non-finite term sets the flag.  Both words start at zero (cudaMemsetAsync).
 __global__ void k_acc_emax(const double* __restrict__ x, const double* __restrict__ y, int64_t n, int* __restrict__ emax,
                            int* __restrict__ nonfinite) {
-  int best = INT_MIN;
+  int best = 0;
   bool bad = false;
   for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT) {
     double v = dterm(x, y, i);
     if (!isfinite(v)) { bad = true; continue; }
-    if (v != 0.0) { int e; frexp(v, &e); best = max(best, e); }
+    if (v != 0.0) { int e; frexp(v, &e); best = max(best, e + kEBias); }
   }
   for (int o = 16; o; o >>= 1) best = max(best, __shfl_down_sync(0xffffffffu, best, o));
-  if ((threadIdx.x & 31) == 0 && best != INT_MIN) atomicMax(emax, best);
+  if ((threadIdx.x & 31) == 0 && best != 0) atomicMax(emax, best);
   if (bad) atomicExch(nonfinite, 1);
 }
 __device__ void block_acc_reduce(Acc192 a, uint64_t* __restrict__ out) {
@@ -140,22 +142,29 @@ __device__ void block_acc_reduce(Acc192 a, uint64_t* __restrict__ out) {
   }
   if (threadIdx.x == 0) for (int k = 0; k < 3; ++k) out[k] = s[k][0];
 }
-// pass 2: fixed-point accumulation, one 192-bit partial per block
+// pass 2: fixed-point accumulation, one 192-bit partial per block (zero when pass 1 found no
+// nonzero term or a non-finite one: the host reports 0 or NaN from the flags)
 __global__ void __launch_bounds__(kT) k_acc_sum(const double* __restrict__ x, const double* __restrict__ y, int64_t n,
-                                                const int* __restrict__ emax, uint64_t* __restrict__ part) {
+                                                const int* __restrict__ flags, uint64_t* __restrict__ part) {
   Acc192 a = {{0, 0, 0}};
-  const int lsb = *emax - kAccFrac;
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT)
-    acc_term(a, dterm(x, y, i), lsb);
+  const int eb = flags[0];
+  if (eb != 0 && flags[1] == 0) {
+    const int lsb = eb - kEBias - kAccFrac;
+    for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT)
+      acc_term(a, dterm(x, y, i), lsb);
+  }
   block_acc_reduce(a, part + 3 * blockIdx.x);
 }
-__global__ void __launch_bounds__(kT) k_acc_final(const uint64_t* __restrict__ part, int nb, uint64_t* __restrict__ out) {
+// pass 3: sum of the block partials into out[0..2]; out[3] carries the flags of pass 1
+__global__ void __launch_bounds__(kT) k_acc_final(const uint64_t* __restrict__ part, int nb, const int* __restrict__ flags,
+                                                  uint64_t* __restrict__ out) {
   Acc192 a = {{0, 0, 0}};
   for (int b = threadIdx.x; b < nb; b += kT) {
     Acc192 t = {{part[3 * b], part[3 * b + 1], part[3 * b + 2]}};
     acc_add(a, t);
   }
   block_acc_reduce(a, out);
+  if (threadIdx.x == 0) out[3] = (uint64_t)(uint32_t)flags[0] | ((uint64_t)(uint32_t)flags[1] << 32);
 }
 // onsite diagonal elements gathered for the exact trace
 __global__ void k_gather_diag(int n_prim, const int64_t* __restrict__ onsite, const int* __restrict__ prim_nsf,
@@ -270,26 +279,41 @@ double acc192_to_double(const uint64_t in[3], int lsb_exp) {
   return neg ? -v : v;
 }
 
-static double exact_sum(System& S, const double* x, const double* y, int64_t n) {
-  if (S.acc_part.n < (size_t)(3 * kRedBlocks + 3)) S.acc_part.alloc(3 * kRedBlocks + 3);
-  if (S.acc_flags.n < 2) S.acc_flags.alloc(2);
-  int init[2] = {INT_MIN, 0};
-  CQ_CUDA(cudaMemcpyAsync(S.acc_flags.p, init, sizeof(init), cudaMemcpyHostToDevice, S.stream));
-  k_acc_emax<<<kRedBlocks, kT, 0, S.stream>>>(x, y, n, S.acc_flags.p, S.acc_flags.p + 1);
-  int flags[2];
-  CQ_CUDA(cudaMemcpyAsync(flags, S.acc_flags.p, sizeof(flags), cudaMemcpyDeviceToHost, S.stream));
-  CQ_CUDA(cudaStreamSynchronize(S.stream));
-  S.launches++;
-  if (flags[1]) return std::numeric_limits<double>::quiet_NaN();
-  if (flags[0] == INT_MIN) return 0.0;
-  k_acc_sum<<<kRedBlocks, kT, 0, S.stream>>>(x, y, n, S.acc_flags.p, S.acc_part.p);
-  k_acc_final<<<1, kT, 0, S.stream>>>(S.acc_part.p, kRedBlocks, S.acc_part.p + 3 * kRedBlocks);
-  S.launches += 2;
+// Grid of the exact sums: integer accumulation is associative, so the grid only sets the
+// parallelism (about four elements per thread, at most 148 SMs x 8 blocks).
+static int acc_grid(int64_t n) {
+  int64_t g = (n + 4 * kT - 1) / (4 * kT);
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, kRedBlocks));
+}
+
+// Enqueue the three passes; the 4-word result (3 fixed-point words, flags) lands in res.
+static void exact_sum_enqueue(System& S, const double* x, const double* y, int64_t n, int* flags, uint64_t* part,
+                              uint64_t* res) {
+  const int g = acc_grid(n);
+  CQ_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(int), S.stream));
+  k_acc_emax<<<g, kT, 0, S.stream>>>(x, y, n, flags, flags + 1);
+  k_acc_sum<<<g, kT, 0, S.stream>>>(x, y, n, flags, part);
+  k_acc_final<<<1, kT, 0, S.stream>>>(part, g, flags, res);
+  S.launches += 3;
   CQ_CUDA(cudaGetLastError());
-  uint64_t w[3];
+}
+
+// Value of a 4-word exact-sum result (k_acc_final layout).
+static double exact_sum_value(const uint64_t r[4]) {
+  const int eb = (int)(uint32_t)(r[3] & 0xffffffffu);
+  if ((r[3] >> 32) != 0) return std::numeric_limits<double>::quiet_NaN();
+  if (eb == 0) return 0.0;
+  return acc192_to_double(r, eb - kEBias - kAccFrac);
+}
+
+static double exact_sum(System& S, const double* x, const double* y, int64_t n) {
+  if (S.acc_part.n < (size_t)(3 * kRedBlocks + 4)) S.acc_part.alloc(3 * kRedBlocks + 4, S.stream);
+  if (S.acc_flags.n < 2) S.acc_flags.alloc(2, S.stream);
+  exact_sum_enqueue(S, x, y, n, S.acc_flags.p, S.acc_part.p, S.acc_part.p + 3 * kRedBlocks);
+  uint64_t w[4];
   CQ_CUDA(cudaMemcpyAsync(w, S.acc_part.p + 3 * kRedBlocks, sizeof(w), cudaMemcpyDeviceToHost, S.stream));
-  CQ_CUDA(cudaStreamSynchronize(S.stream));
-  return acc192_to_double(w, flags[0] - kAccFrac);
+  host_wait(S);
+  return exact_sum_value(w);
 }
 
 double dev_dot(System& S, const double* x, const double* y, int64_t n) { return exact_sum(S, x, y, n); }
@@ -301,7 +325,7 @@ double dev_trace(System& S, int r, const double* a) {
     std::vector<int> off(N + 1, 0);
     for (int p = 0; p < N; ++p) off[p + 1] = off[p] + S.geo.nsf[S.geo.prim_global[p]];
     S.diag_off.upload(off, S.stream);
-    S.diag_buf.alloc(std::max(off[N], 1));
+    S.diag_buf.alloc(std::max(off[N], 1), S.stream);
   }
   k_gather_diag<<<(N + kT - 1) / kT, kT, 0, S.stream>>>(N, R.onsite.p, S.dg.prim_nsf.p, S.diag_off.p, a, S.diag_buf.p);
   S.launches++;
@@ -312,7 +336,7 @@ void dev_h_limits(System& S, int r, const double* h, double* hmin, double* hmax)
   RangeIndex& R = *S.ranges[r];
   int N = S.geo.n_prim;
   DevBuf<double> mn, mx, out;
-  mn.alloc(N); mx.alloc(N); out.alloc(2);
+  mn.alloc(N, S.stream); mx.alloc(N, S.stream); out.alloc(2, S.stream);
   k_hlimits<<<(N * 32 + kT - 1) / kT, kT, 0, S.stream>>>(N, R.row_ptr.p, R.nb_elem.p, R.nb_cover.p, R.onsite.p,
                                                        S.dg.prim_nsf.p, S.dg.cover_nsf.p, h, mn.p, mx.p);
   k_minmax<<<1, kT, 0, S.stream>>>(mn.p, mx.p, N, out.p);
@@ -320,7 +344,7 @@ void dev_h_limits(System& S, int r, const double* h, double* hmin, double* hmax)
   CQ_CUDA(cudaGetLastError());
   double o[2];
   CQ_CUDA(cudaMemcpyAsync(o, out.p, sizeof(o), cudaMemcpyDeviceToHost, S.stream));
-  CQ_CUDA(cudaStreamSynchronize(S.stream));
+  host_wait(S);
   *hmin = o[0];
   *hmax = o[1];
 }

@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cstring>
 #include <functional>
+#include <mutex>
 #include <numeric>
 #include <string>
 
@@ -12,11 +13,45 @@ namespace cqb {
 static thread_local std::string g_last_error = "";
 void set_last_error(const std::string& m) { g_last_error = m; }
 
+static thread_local DevAccount t_account;
+DevAccount& dev_account() { return t_account; }
+void dev_account_add(int64_t bytes) {
+  t_account.live += bytes;
+  if (t_account.live > t_account.peak) t_account.peak = t_account.live;
+}
+
+// Keep freed blocks of the device's default pool cached in the process (release threshold =
+// unlimited) so stream-ordered reallocation does not go back to the driver at every
+// synchronisation.  A property of this process's pool only; it ends with the process.
+void init_device_pool() {
+  int dev = 0;
+  CQ_CUDA(cudaGetDevice(&dev));
+  static std::mutex mu;
+  static std::vector<int> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+  cudaMemPool_t pool;
+  CQ_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t thr = UINT64_MAX;
+  CQ_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  done.push_back(dev);
+}
+
 System::~System() {
-  plans.clear();
-  addmaps.clear();
-  ranges.clear();
-  if (own_stream && own) cudaStreamDestroy(own);
+  // buffers may have been used on a stream given with cq_system_set_stream: finish that work
+  // before they are released (on the stream recorded at their allocation)
+  if (stream) cudaStreamSynchronize(stream);
+  if (sync_ev) cudaEventDestroy(sync_ev);
+}
+
+void host_wait(System& S) {
+  if (!S.blocking_sync) {
+    CQ_CUDA(cudaStreamSynchronize(S.stream));
+    return;
+  }
+  if (!S.sync_ev) CQ_CUDA(cudaEventCreateWithFlags(&S.sync_ev, cudaEventBlockingSync | cudaEventDisableTiming));
+  CQ_CUDA(cudaEventRecord(S.sync_ev, S.stream));
+  CQ_CUDA(cudaEventSynchronize(S.sync_ev));
 }
 
 // drop-in kernels (one m_kern_max / m_kern_min call): explicit offsets prepared on the host
@@ -78,9 +113,9 @@ int cq_system_create(int n_atoms, const double* coords, const double* cell, cons
     for (int i = 0; i < n_atoms; ++i) CQ_CHECK(nsf[i] >= 1 && nsf[i] <= 16, CQ_ERR_ARG, "block sizes must be 1..16");
     auto sys = std::make_unique<cq_system>();
     System& S = sys->S;
-    CQ_CUDA(cudaStreamCreateWithFlags(&S.stream, cudaStreamNonBlocking));
-    S.own = S.stream;
-    S.own_stream = true;
+    init_device_pool();
+    CQ_CUDA(cudaStreamCreateWithFlags(&S.own.s, cudaStreamNonBlocking));
+    S.stream = S.own.s;
     GeometryParams prm;
     prm.max_atoms_part = max_atoms_part > 0 ? max_atoms_part : 34;
     prm.gap_threshold = gap_threshold;
@@ -157,9 +192,9 @@ int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, doub
     CQ_CHECK(a && b && c, CQ_ERR_ARG, "null operand");
     System& S = sys->S;
     int64_t la = S.ranges[ra]->length, lb = S.ranges[rb]->length, lc = S.ranges[rc]->length;
-    if (sys->ha.n < (size_t)std::max<int64_t>(la, 1)) sys->ha.alloc(std::max<int64_t>(la, 1));
-    if (sys->hb.n < (size_t)std::max<int64_t>(lb, 1)) sys->hb.alloc(std::max<int64_t>(lb, 1));
-    if (sys->hc.n < (size_t)std::max<int64_t>(lc, 1)) sys->hc.alloc(std::max<int64_t>(lc, 1));
+    if (sys->ha.n < (size_t)std::max<int64_t>(la, 1)) sys->ha.alloc(std::max<int64_t>(la, 1), sys->S.stream);
+    if (sys->hb.n < (size_t)std::max<int64_t>(lb, 1)) sys->hb.alloc(std::max<int64_t>(lb, 1), sys->S.stream);
+    if (sys->hc.n < (size_t)std::max<int64_t>(lc, 1)) sys->hc.alloc(std::max<int64_t>(lc, 1), sys->S.stream);
     ProductPlan& P = get_plan(S, mult_type, ra, rb, rc);
     if (mult_type == 1) CQ_CUDA(cudaMemcpyAsync(sys->ha.p, a, la * sizeof(double), cudaMemcpyHostToDevice, S.stream));
     CQ_CUDA(cudaMemcpyAsync(sys->hb.p, b, lb * sizeof(double), cudaMemcpyHostToDevice, S.stream));
@@ -217,7 +252,7 @@ int cq_system_set_stream(cq_system* sys, void* stream) {
   return guarded([&] {
     check_sys(sys);
     CQ_CUDA(cudaStreamSynchronize(sys->S.stream));
-    sys->S.stream = stream ? (cudaStream_t)stream : sys->S.own;
+    sys->S.stream = stream ? (cudaStream_t)stream : sys->S.own.s;
   });
 }
 
@@ -253,9 +288,19 @@ int cq_system_set_option(cq_system* sys, int option, int value) {
     if (option == CQ_OPT_MULT_VARIANT) {
       CQ_CHECK(value == 0 || value == 1, CQ_ERR_ARG, "mult variant must be 0 or 1");
       sys->S.mult_variant = value;
+    } else if (option == CQ_OPT_BLOCKING_SYNC) {
+      sys->S.blocking_sync = value != 0;
     } else {
       throw Error(CQ_ERR_ARG, "unknown option");
     }
+  });
+}
+
+int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, r);
+    CQ_CHECK(out && (which == 0 || which == 1), CQ_ERR_ARG, "bad generator arguments");
+    generate_SH(sys->S, r, which, seed, out);
   });
 }
 

@@ -30,7 +30,7 @@ DMat LNVSolver::temp(int rng) {
   if (!fl.empty()) { p = fl.back(); fl.pop_back(); }
   else {
     pool_.emplace_back();
-    pool_.back().alloc(std::max<int64_t>(S.ranges[r]->length, 1));
+    pool_.back().alloc(std::max<int64_t>(S.ranges[r]->length, 1), S.stream);
     p = pool_.back().p;
   }
   CQ_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * std::max<int64_t>(S.ranges[r]->length, 1), S.stream));
@@ -140,13 +140,13 @@ void LNVSolver::set_identity_onsite(DMat& A) {
   std::vector<int64_t> ons = S.ranges[R[A.rng]]->onsite.download(S.stream);
   std::vector<double> h(A.n, 0.0);
   CQ_CUDA(cudaMemcpyAsync(h.data(), A.p, sizeof(double) * A.n, cudaMemcpyDeviceToHost, S.stream));
-  CQ_CUDA(cudaStreamSynchronize(S.stream));
+  host_wait(S);
   for (int p = 0; p < S.geo.n_prim; ++p) {
     int nd = S.geo.nsf[S.geo.prim_global[p]];
     for (int j = 0; j < nd; ++j) h[ons[p] + j * nd + j] = 1.0;
   }
   CQ_CUDA(cudaMemcpyAsync(A.p, h.data(), sizeof(double) * A.n, cudaMemcpyHostToDevice, S.stream));
-  CQ_CUDA(cudaStreamSynchronize(S.stream));
+  host_wait(S);
 }
 
 // ---------------------------------------------------------------------------
@@ -166,7 +166,7 @@ LNVSolver::LNVSolver(System& sys, const int ranges[NR], double ne_spin, const cq
 DMat LNVSolver::own(int rng) {
   owned_.emplace_back();
   int64_t n = S.ranges[R[rng]]->length;
-  owned_.back().alloc(std::max<int64_t>(n, 1));
+  owned_.back().alloc(std::max<int64_t>(n, 1), S.stream);
   CQ_CUDA(cudaMemsetAsync(owned_.back().p, 0, sizeof(double) * std::max<int64_t>(n, 1), S.stream));
   return DMat{rng, owned_.back().p, n, nullptr};
 }
@@ -248,7 +248,7 @@ double LNVSolver::invert_S() {
   {
     std::vector<double> hS(Smat.n);
     CQ_CUDA(cudaMemcpyAsync(hS.data(), Smat.p, sizeof(double) * Smat.n, cudaMemcpyDeviceToHost, S.stream));
-    CQ_CUDA(cudaStreamSynchronize(S.stream));
+    host_wait(S);
     RangeIndex& RI = *S.ranges[R[RS]];
     std::vector<int> cov = RI.nb_cover.download(S.stream);
     std::vector<int64_t> el = RI.nb_elem.download(S.stream);

@@ -39,34 +39,57 @@ void set_last_error(const std::string& m);
 
 // ---------------------------------------------------------------------------
 // device buffer (RAII, stream-ordered allocator)
+// Memory comes from the device's default pool with cudaMallocAsync on the stream
+// given to alloc() and goes back with cudaFreeAsync on that stream, so neither
+// allocation nor release synchronises the device: solves of independent systems
+// on their own streams keep running while another one sets up or tears down.
+// A buffer is released on the stream it was (last) allocated on; every buffer is
+// used on that stream or on a later stream of the same system, which is
+// synchronised before the system (or solver) holding it is destroyed.
 // ---------------------------------------------------------------------------
+struct DevAccount {               // device bytes held through DevBuf by the calling thread
+  int64_t live = 0, peak = 0;
+};
+DevAccount& dev_account();        // thread-local
+void dev_account_add(int64_t bytes);
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t st = nullptr;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), st(o.st) { o.p = nullptr; o.n = 0; }
   DevBuf& operator=(DevBuf&& o) noexcept {
-    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    if (this != &o) { release(); p = o.p; n = o.n; st = o.st; o.p = nullptr; o.n = 0; }
     return *this;
   }
   ~DevBuf() { release(); }
-  void alloc(size_t count) {
+  // (re)allocate on stream s; old memory is released on s, the stream any pending use is on
+  void alloc(size_t count, cudaStream_t s) {
+    st = s;
     release();
-    n = count;
     if (count) {
-      cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-      if (e != cudaSuccess) { p = nullptr; n = 0; throw Error(CQ_ERR_OOM, "cudaMalloc failed: " + std::string(cudaGetErrorString(e))); }
+      cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), s);
+      if (e != cudaSuccess) {
+        p = nullptr;
+        throw Error(CQ_ERR_OOM, "cudaMallocAsync failed: " + std::string(cudaGetErrorString(e)));
+      }
+      n = count;
+      dev_account_add((int64_t)(count * sizeof(T)));
     }
   }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      cudaFreeAsync(p, st);
+      dev_account_add(-(int64_t)(n * sizeof(T)));
+    }
     p = nullptr; n = 0;
   }
   void upload(const T* h, size_t count, cudaStream_t s) {
-    alloc(count);
+    alloc(count, s);
     if (count) CQ_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
   }
   void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
@@ -141,6 +164,7 @@ struct DevGeometry {
   DevBuf<double> prim_x, cover_x;
   DevBuf<int> prim_nsf, prim_cover_label, prim_seq, prim_part, part_disp, cover_nsf, cover_part, cover_seq,
       cover_label_of_part, label_to_cover, cover_first, cover_home_prim, part_first_prim;
+  DevBuf<int> prim_global, cover_global, cover_shift;   // uploaded on first use (input generators)
 };
 
 struct RangeIndex {
@@ -209,7 +233,15 @@ struct ProductProfile {
   ~ProductProfile();
 };
 
+struct OwnedStream {              // destroyed after every buffer of the system has been released on it
+  cudaStream_t s = nullptr;
+  ~OwnedStream() {
+    if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+  }
+};
+
 struct System {
+  OwnedStream own;                // the stream created with the system (first member: destroyed last)
   Geometry geo;
   DevGeometry dg;
   std::vector<std::unique_ptr<RangeIndex>> ranges;
@@ -217,9 +249,7 @@ struct System {
   std::map<std::pair<int, int>, std::unique_ptr<AddMap>> addmaps;
   std::map<std::tuple<int, int, int, int>, std::unique_ptr<MixedPlan>> mplans;
   std::map<std::pair<int, int>, FragBuf> frags;   // (range, slot) fragment buffers of the mixed products
-  cudaStream_t stream = nullptr;
-  cudaStream_t own = nullptr;     // the stream created with the system
-  bool own_stream = false;
+  cudaStream_t stream = nullptr;  // the stream all work of the system is enqueued on
   int uniform_nsf = 0;            // block size when every atom has the same one, else 0
   DevBuf<double> red_scratch;     // scratch of the min/max reductions
   DevBuf<uint64_t> acc_part;      // 192-bit partials of the exact sums
@@ -228,9 +258,14 @@ struct System {
   DevBuf<double> diag_buf;        // gathered onsite diagonal (exact trace)
   int64_t launches = 0;           // kernels launched by this system (all kinds)
   int mult_variant = 1;           // 4x4 FP64 product kernel: 0 = one lane per element, 1 = one thread per block
+  bool blocking_sync = false;     // host waits sleep on a blocking-sync event instead of spinning
+  cudaEvent_t sync_ev = nullptr;
   ProductProfile prof;
   ~System();
 };
+
+void init_device_pool();          // once per device: cache freed pool memory in the process
+void host_wait(System& S);        // wait for all work enqueued on S.stream
 
 // index.cu
 void upload_geometry(System& S);
@@ -243,6 +278,9 @@ MixedPlan& get_mixed_plan(System& S, int mult_type, int ra, int rb, int rc);
 
 // mult.cu
 void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, double* c, int exact);
+
+// gen.cu: synthetic S (which = 0) or H (which = 1) of range r into out
+void generate_SH(System& S, int r, int which, uint64_t seed, double* out);
 
 // mixed.cu
 void to_fragments(System& S, int r, const double* src, int role_b, int trans, uint4* hi, uint4* lo);

@@ -385,7 +385,7 @@ template <class Tin>
 int64_t exclusive_scan(const Tin* in, int64_t n, int64_t* out, cudaStream_t st) {
   int nb = (int)std::max<int64_t>(1, (n + 255) / 256);
   DevBuf<int64_t> sums;
-  sums.alloc(nb + 1);
+  sums.alloc(nb + 1, st);
   if (n > 0) k_scan_blocks<Tin><<<nb, 256, 0, st>>>(in, n, out, sums.p);
   else CQ_CUDA(cudaMemsetAsync(sums.p, 0, sizeof(int64_t), st));
   k_scan_sums<<<1, 1024, 0, st>>>(sums.p, n > 0 ? nb : 0, out + n);
@@ -449,27 +449,27 @@ void build_range_index(System& S, RangeIndex& R) {
   const int T = 256, WPB = T / kWarp;
   // ---- neighbour counts and offsets
   DevBuf<int> row_cnt;
-  row_cnt.alloc(N);
+  row_cnt.alloc(N, st);
   DevBuf<int64_t> row_len, ptr64;
-  row_len.alloc(N);
-  ptr64.alloc(N + 1);
+  row_len.alloc(N, st);
+  ptr64.alloc(N + 1, st);
   k_naba_count<<<nblk(N, WPB), T, 0, st>>>(N, NC, d.prim_x.p, d.cover_x.p, d.prim_nsf.p, d.cover_nsf.p, thr, row_cnt.p,
                                           row_len.p);
   CQ_CUDA(cudaGetLastError());
   int64_t nnz = exclusive_scan(row_cnt.p, N, ptr64.p, st);
   CQ_CHECK(nnz < (int64_t)INT32_MAX, CQ_ERR_ARG, "too many blocks for 32-bit block ids");
   R.nnz = (int)nnz;
-  R.row_ptr.alloc(N + 1);
+  R.row_ptr.alloc(N + 1, st);
   k_i64_to_i32<<<nblk(N + 1, T), T, 0, st>>>(ptr64.p, N + 1, R.row_ptr.p);
-  R.row_elem.alloc(N + 1);
+  R.row_elem.alloc(N + 1, st);
   R.length = exclusive_scan(row_len.p, N, R.row_elem.p, st);
   // ---- fill
-  R.nb_cover.alloc(std::max(R.nnz, 1));
-  R.nb_elem.alloc(std::max(R.nnz, 1));
-  R.nb_row.alloc(std::max(R.nnz, 1));
-  R.nb_ibpart.alloc(std::max(R.nnz, 1));
-  R.nb_radius.alloc(std::max(R.nnz, 1));
-  R.onsite.alloc(N);
+  R.nb_cover.alloc(std::max(R.nnz, 1), st);
+  R.nb_elem.alloc(std::max(R.nnz, 1), st);
+  R.nb_row.alloc(std::max(R.nnz, 1), st);
+  R.nb_ibpart.alloc(std::max(R.nnz, 1), st);
+  R.nb_radius.alloc(std::max(R.nnz, 1), st);
+  R.onsite.alloc(N, st);
   CQ_CUDA(cudaMemsetAsync(R.onsite.p, 0xff, sizeof(int64_t) * N, st));
   k_naba_fill<<<nblk(N, WPB), T, 0, st>>>(N, NC, d.prim_x.p, d.cover_x.p, d.prim_nsf.p, d.cover_nsf.p, d.cover_part.p,
                                          d.cover_seq.p, d.cover_label_of_part.p, d.prim_cover_label.p, d.prim_seq.p,
@@ -479,20 +479,20 @@ void build_range_index(System& S, RangeIndex& R) {
   CQ_CUDA(cudaGetLastError());
   // ---- halo
   DevBuf<int> flag;
-  flag.alloc(NC);
+  flag.alloc(NC, st);
   CQ_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int) * NC, st));
   if (R.nnz) k_flag<<<nblk(R.nnz, T), T, 0, st>>>(R.nnz, R.nb_cover.p, flag.p);
   DevBuf<int64_t> hex;
-  hex.alloc(NC + 1);
+  hex.alloc(NC + 1, st);
   int64_t nh = exclusive_scan(flag.p, NC, hex.p, st);
   R.ni_in_halo = (int)nh;
   DevBuf<int> hex32;
-  hex32.alloc(NC + 1);
+  hex32.alloc(NC + 1, st);
   k_i64_to_i32<<<nblk(NC + 1, T), T, 0, st>>>(hex.p, NC + 1, hex32.p);
-  R.cover_to_halo.alloc(NC);
-  R.halo_cover.alloc(std::max<int64_t>(nh, 1));
+  R.cover_to_halo.alloc(NC, st);
+  R.halo_cover.alloc(std::max<int64_t>(nh, 1), st);
   k_halo_number<<<nblk(NC, T), T, 0, st>>>(NC, flag.p, hex32.p, R.cover_to_halo.p, R.halo_cover.p);
-  R.nb_halo.alloc(std::max(R.nnz, 1));
+  R.nb_halo.alloc(std::max(R.nnz, 1), st);
   if (R.nnz) k_gather_int<<<nblk(R.nnz, T), T, 0, st>>>(R.nnz, R.nb_cover.p, R.cover_to_halo.p, R.nb_halo.p);
   CQ_CUDA(cudaGetLastError());
   // halo partitions (host bookkeeping of np_in_halo from the flags)
@@ -508,24 +508,24 @@ void build_range_index(System& S, RangeIndex& R) {
   }
   // ---- retro lists
   DevBuf<int> err;
-  err.alloc(1);
+  err.alloc(1, st);
   CQ_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), st));
   DevBuf<int> col_cnt;
-  col_cnt.alloc(std::max<int64_t>(nh, 1));
+  col_cnt.alloc(std::max<int64_t>(nh, 1), st);
   DevBuf<int64_t> col64;
-  col64.alloc(nh + 1);
+  col64.alloc(nh + 1, st);
   if (nh) k_retr_count<<<nblk(nh, WPB), T, 0, st>>>((int)nh, N, R.halo_cover.p, d.cover_x.p, d.prim_x.p, thr, col_cnt.p);
   int64_t ncol = exclusive_scan(col_cnt.p, nh, col64.p, st);
   CQ_CHECK(ncol == nnz, CQ_ERR_STATE, "retro lists disagree with the neighbour lists");
-  R.col_ptr.alloc(nh + 1);
+  R.col_ptr.alloc(nh + 1, st);
   k_i64_to_i32<<<nblk(nh + 1, T), T, 0, st>>>(col64.p, (int)nh + 1, R.col_ptr.p);
-  R.col_row.alloc(std::max(R.nnz, 1));
-  R.col_blk.alloc(std::max(R.nnz, 1));
+  R.col_row.alloc(std::max(R.nnz, 1), st);
+  R.col_blk.alloc(std::max(R.nnz, 1), st);
   if (nh)
     k_retr_fill<<<nblk(nh, WPB), T, 0, st>>>((int)nh, N, R.halo_cover.p, d.cover_x.p, d.prim_x.p, thr, R.col_ptr.p,
                                              R.row_ptr.p, R.nb_cover.p, R.col_row.p, R.col_blk.p, err.p);
   // ---- transpose destinations
-  R.trans_dest.alloc(std::max(R.nnz, 1));
+  R.trans_dest.alloc(std::max(R.nnz, 1), st);
   if (R.nnz)
     k_trans_dest<<<nblk(R.nnz, T), T, 0, st>>>(R.nnz, R.nb_row.p, R.nb_cover.p, d.cover_part.p, d.cover_label_of_part.p,
                                                d.cover_home_prim.p, d.prim_cover_label.p, d.prim_seq.p, d.label_to_cover.p,
@@ -564,24 +564,24 @@ ProductPlan& get_plan(System& S, int mult_type, int ra, int rb, int rc) {
   P.out_range = mult_type == 1 ? rc : ra;
   int nout = out.nnz;
   DevBuf<int> cnt, err;
-  cnt.alloc(std::max(nout, 1));
-  err.alloc(1);
+  cnt.alloc(std::max(nout, 1), st);
+  err.alloc(1, st);
   DevBuf<unsigned long long> fl;
-  fl.alloc(1);
+  fl.alloc(1, st);
   CQ_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * std::max(nout, 1), st));
   CQ_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), st));
   CQ_CUDA(cudaMemsetAsync(fl.p, 0, sizeof(unsigned long long), st));
   if (mult_type == 1) k_plan1<<<nblk(N, WPB), T, 0, st>>>(pa, N, 0, cnt.p, nullptr, nullptr, nullptr, fl.p, err.p);
   else if (nout) k_plan2<<<nblk(nout, WPB), T, 0, st>>>(pa, nout, 0, cnt.p, nullptr, nullptr, fl.p, err.p);
   CQ_CUDA(cudaGetLastError());
-  P.ptr.alloc(nout + 1);
+  P.ptr.alloc(nout + 1, st);
   P.n_pairs = exclusive_scan(cnt.p, nout, P.ptr.p, st);
   CQ_CHECK(read_flag(err.p, st) == 0, CQ_ERR_BOUNDS, "pair list: neighbour partition outside the covering set");
   unsigned long long hfl = 0;
   CQ_CUDA(cudaMemcpyAsync(&hfl, fl.p, sizeof(hfl), cudaMemcpyDeviceToHost, st));
   CQ_CUDA(cudaStreamSynchronize(st));
   P.flops = (int64_t)hfl;
-  P.pairs.alloc(std::max<int64_t>(P.n_pairs, 1));
+  P.pairs.alloc(std::max<int64_t>(P.n_pairs, 1), st);
   if (mult_type == 1) {
     CQ_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * std::max(nout, 1), st));
     k_plan1<<<nblk(N, WPB), T, 0, st>>>(pa, N, 1, nullptr, P.ptr.p, cnt.p, P.pairs.p, nullptr, err.p);
@@ -623,14 +623,14 @@ MixedPlan& get_mixed_plan(System& S, int mult_type, int ra, int rb, int rc) {
     pa.ng_cover = S.geo.ng_cover;
     const int nout = A.nnz, T = 256, WPB = T / kWarp;
     DevBuf<int> cnt;
-    cnt.alloc(std::max(nout, 1));
+    cnt.alloc(std::max(nout, 1), st);
     const int* g = S.geo.ncover;
     if (nout) k_plan2x<<<nblk(nout, WPB), T, 0, st>>>(pa, nout, 0, d.prim_cover_label.p, g[0], g[1], g[2], cnt.p, nullptr, nullptr);
     CQ_CUDA(cudaGetLastError());
-    M.own_ptr.alloc(nout + 1);
+    M.own_ptr.alloc(nout + 1, st);
     int64_t np2 = exclusive_scan(cnt.p, nout, M.own_ptr.p, st);
     CQ_CHECK(np2 == P.n_pairs, CQ_ERR_STATE, "type-2 lists by input block disagree with the default-order lists");
-    M.own_pairs.alloc(std::max<int64_t>(np2, 1));
+    M.own_pairs.alloc(std::max<int64_t>(np2, 1), st);
     if (nout) k_plan2x<<<nblk(nout, WPB), T, 0, st>>>(pa, nout, 1, d.prim_cover_label.p, g[0], g[1], g[2], nullptr, M.own_ptr.p, M.own_pairs.p);
     CQ_CUDA(cudaGetLastError());
     M.ptr = M.own_ptr.p;
@@ -654,7 +654,7 @@ AddMap& get_addmap(System& S, int ra, int rb) {
   if (it != S.addmaps.end()) return *it->second;
   RangeIndex &A = *S.ranges[ra], &B = *S.ranges[rb];
   auto m = std::make_unique<AddMap>();
-  m->partner.alloc(std::max(A.nnz, 1));
+  m->partner.alloc(std::max(A.nnz, 1), S.stream);
   if (A.nnz) k_addmap<<<nblk(A.nnz, 256), 256, 0, S.stream>>>(A.nnz, A.nb_row.p, A.nb_cover.p, B.row_ptr.p, B.nb_cover.p, m->partner.p);
   CQ_CUDA(cudaGetLastError());
   auto res = S.addmaps.emplace(key, std::move(m));

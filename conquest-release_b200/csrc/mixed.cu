@@ -179,7 +179,7 @@ void to_fragments(System& S, int r, const double* src, int role_b, int trans, ui
 static FragBuf& frag_buffer(System& S, int r, int slot) {
   FragBuf& f = S.frags[std::make_pair(r, slot)];
   size_t need = (size_t)std::max(S.ranges[r]->nnz, 1) * 32;
-  if (f.hi.n < need) { f.hi.alloc(need); f.lo.alloc(need); }
+  if (f.hi.n < need) { f.hi.alloc(need, S.stream); f.lo.alloc(need, S.stream); }
   return f;
 }
 

@@ -162,9 +162,20 @@ int cq_profile_read(cq_system* sys, int64_t* launches, double* ms, double* bytes
 /* Kernels launched by this system so far (all kinds). */
 int cq_launch_count(cq_system* sys, int64_t* count);
 
+/* Synthetic input generator (no counterpart in the reference, whose S and H come from grid
+ * integration): writes S (which = 0: onsite identity, offsite 0.3 exp(-r/2)) or H (which = 1:
+ * onsite diagonal -0.5 u(seed, atom, orbital), offsite -0.2 exp(-r/2)) of range r into the device
+ * array `out` (range length), stream-ordered.  Same values as cq_b200.inputs.overlap_S /
+ * hamiltonian_H up to the last bit of exp(). */
+int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out);
+
 /* Tuning options.  CQ_OPT_MULT_VARIANT: FP64 4x4 product kernel, 0 = one lane per output
- * element, 1 = one thread per output block (default).  Both give identical results. */
+ * element, 1 = one thread per output block (default).  Both give identical results.
+ * CQ_OPT_BLOCKING_SYNC: 1 = the host thread sleeps on a blocking-sync event whenever the
+ * solver waits for a scalar from the device (many concurrent solvers per host core), 0 = it
+ * spins in cudaStreamSynchronize (default, lowest latency for one solver). */
 #define CQ_OPT_MULT_VARIANT 1
+#define CQ_OPT_BLOCKING_SYNC 2
 int cq_system_set_option(cq_system* sys, int option, int value);
 
 /* ------------------------------------------------------------------------ */
@@ -241,6 +252,72 @@ int cq_lnv_solve(cq_lnv* s, cq_lnv_result* res);
  * end-to-end call of a user holding S and H in host memory.
  */
 int cq_lnv_solve_host(cq_lnv* s, const double* S, const double* H, double* L_out, double* K_out, cq_lnv_result* res);
+
+/* ------------------------------------------------------------------------ */
+/* Serving loop: continuous batching of independent density-matrix solves    */
+/* (no counterpart in the reference, which solves one system per run).       */
+/* ------------------------------------------------------------------------ */
+/*
+ * A server owns `n_slots` worker threads, each with its own non-blocking CUDA stream on the
+ * device current at creation.  Submitted requests queue in arrival order; a free slot admits the
+ * first queued request whose memory estimate fits into what `hbm_budget` leaves after the
+ * admitted ones (a request overtaken `max_bypass` times blocks later ones until it fits; one that
+ * exceeds the whole budget runs alone).  An admitted request keeps its geometry, indices, S, H,
+ * L and every temporary on the device from index build to result: S and H come from the
+ * synthetic generators of cq_generate_SH with the request's seed, then cq_lnv_solve runs with
+ * the server's parameters (`mixed` per request).  Solves of different slots overlap on the
+ * device; each result is bit-identical to the same solve run alone (all reductions are exact
+ * and every kernel is deterministic).  Times are seconds since the server was created.
+ */
+typedef struct {
+  int n_slots;             /* concurrent solves (1..64) */
+  int64_t hbm_budget;      /* bytes the admitted requests' estimates may hold together */
+  int max_bypass;          /* times a queued request may be overtaken by later, smaller ones */
+  int blocking_sync;       /* host waits sleep (CQ_OPT_BLOCKING_SYNC) */
+  int dry_run;             /* 1: no device work; a request holds its slot and budget for
+                              dry_run_seconds (scheduler tests without a GPU) */
+  double dry_run_seconds;
+  cq_lnv_params lnv;       /* solver parameters of every request (lnv.mixed is overridden) */
+} cq_server_config;
+
+typedef struct {
+  int n_atoms;
+  const double* coords;    /* 3*n_atoms, bohr (copied at submit) */
+  const double* cell;      /* 3 orthorhombic cell lengths */
+  const int* nsf;          /* n_atoms block sizes */
+  double rs, rh, rl, rt;   /* S, H, L and T ranges; the chain's other ranges follow (dimens_module) */
+  double ne_spin;          /* electrons per spin channel */
+  uint64_t seed;           /* S/H generator seed */
+  int mixed;               /* 1: split-precision phase first (cq_lnv_params.mixed) */
+  double t_arrival;        /* arrival time on the server clock (< 0: the time of submission) */
+} cq_request;
+
+typedef struct {
+  int64_t id;
+  int status;              /* CQ_OK or the CQ_ERR_* code of the failed solve */
+  int n_atoms, converged, mixed, slot;
+  double energy, electrons, residual;
+  int64_t n_products, flops, n_products_mixed, flops_mixed;
+  double t_arrival, t_admit, t_done;    /* latency = t_done - t_arrival */
+  int64_t bytes_estimate;  /* admission estimate */
+  int64_t bytes_peak;      /* device bytes the solve actually held at its peak */
+  char message[128];       /* error message when status != CQ_OK */
+} cq_request_result;
+
+typedef struct cq_server cq_server;
+int cq_server_config_default(cq_server_config* c);
+int cq_server_create(const cq_server_config* c, cq_server** out);
+/* Queue a request; *id identifies its result.  Returns immediately. */
+int cq_server_submit(cq_server* s, const cq_request* r, int64_t* id);
+/* Wait up to timeout_s (< 0: forever) for the result of `id` and remove it from the server;
+ * CQ_ERR_TIMEOUT if it is not finished by then. */
+int cq_server_wait(cq_server* s, int64_t id, double timeout_s, cq_request_result* out);
+/* Seconds on the server clock. */
+int cq_server_now(cq_server* s, double* t);
+/* Memory estimate the admission uses for a request (bytes). */
+int cq_request_estimate(const cq_request* r, int64_t* bytes);
+/* Stop accepting work, finish what is queued or running, join the workers. */
+int cq_server_destroy(cq_server* s);
 
 #ifdef __cplusplus
 }

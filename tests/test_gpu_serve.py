@@ -1,0 +1,97 @@
+"""Serving loop on the GPU: every result is the same alone and in the mix.
+
+Each solve is deterministic (exact reductions, fixed kernels), so the energy, electron count and
+work of a request are compared bit for bit between a one-slot server (requests run one after
+another) and a four-slot server (all requests overlap on the device), and against the direct
+LNV entry point fed with the same device-generated S and H.
+"""
+import numpy as np
+import pytest
+
+import cq_b200
+from cq_b200 import inputs
+
+pytestmark = pytest.mark.gpu
+
+RANGES = (8.0, 9.0, 10.0, 8.0)
+
+
+def _requests():
+    out = []
+    c, cell = inputs.si_cluster(40, sigma=0.1, seed=11)
+    out.append((c, cell, 4, float(len(c)), 101, False))
+    c, cell = inputs.diamond_si(2, sigma=0.1, seed=12)
+    out.append((c, cell, 4, float(len(c)), 102, False))
+    c, cell = inputs.si_cluster(30, sigma=0.1, seed=13)
+    out.append((c, cell, 13, 2.0 * len(c), 103, False))
+    c, cell = inputs.si_cluster(52, sigma=0.1, seed=14)
+    out.append((c, cell, 4, float(len(c)), 104, True))
+    c, cell = inputs.diamond_si(1, sigma=0.1, seed=15)
+    out.append((c, cell, 13, 2.0 * len(c), 105, True))
+    return out
+
+
+def _run(server, reqs):
+    ids = [server.submit(c, cell, nsf, *RANGES, ne, seed=seed, mixed=mx) for c, cell, nsf, ne, seed, mx in reqs]
+    return [server.wait(i, timeout=600) for i in ids]
+
+
+def _key(r):
+    return (r["energy"], r["electrons"], r["n_products"], r["flops"], r["n_products_mixed"], r["converged"])
+
+
+def test_alone_equals_mix():
+    reqs = _requests()
+    alone = cq_b200.Server(n_slots=1)
+    ra = _run(alone, reqs)
+    alone.close()
+    mix = cq_b200.Server(n_slots=4)
+    rm = _run(mix, reqs)
+    mix.close()
+    for a, m in zip(ra, rm):
+        assert a["status"] == 0 and m["status"] == 0, (a["message"], m["message"])
+        assert a["converged"] == 1
+        assert _key(a) == _key(m)
+    # the four-slot run overlapped solves
+    ev = sorted([(r["t_admit"], 1) for r in rm] + [(r["t_done"], -1) for r in rm])
+    cur = best = 0
+    for _, d in ev:
+        cur += d
+        best = max(best, cur)
+    assert best >= 2
+    for r in ra + rm:
+        assert 0 < r["bytes_peak"] <= r["bytes_estimate"]
+
+
+def test_server_equals_direct_solver():
+    import torch
+    c, cell, nsf, ne, seed, mixed = _requests()[1]
+    srv = cq_b200.Server(n_slots=2)
+    r = _run(srv, [(c, cell, nsf, ne, seed, mixed)])[0]
+    srv.close()
+    rng = cq_b200.lnv_ranges(*RANGES)
+    g = cq_b200.System(c, cell, np.full(len(c), nsf, np.int32), list(rng.values()))
+    ridx = {n: i for i, n in enumerate(rng)}
+    S = torch.zeros(g.length(ridx["S"]), dtype=torch.float64, device="cuda")
+    H = torch.zeros(g.length(ridx["H"]), dtype=torch.float64, device="cuda")
+    g.generate_SH(ridx["S"], 0, seed, S)
+    g.generate_SH(ridx["H"], 1, seed, H)
+    g.synchronize()
+    lnv = cq_b200.LNV(g, ridx, ne)
+    lnv.set_SH(S, H)
+    d = lnv.solve()
+    assert (d["energy"], d["electrons"], d["n_products"]) == (r["energy"], r["electrons"], r["n_products"])
+
+
+def test_mixed_request_accuracy():
+    """Split-precision phase then FP64 continuation: same minimum as the FP64 solve within 1e-8 Ha/atom."""
+    c, cell = inputs.diamond_si(2, sigma=0.1, seed=16)
+    n = len(c)
+    srv = cq_b200.Server(n_slots=2)
+    fp = _run(srv, [(c, cell, 13, 2.0 * n, 7, False)])[0]
+    mx = _run(srv, [(c, cell, 13, 2.0 * n, 7, True)])[0]
+    srv.close()
+    assert fp["converged"] == 1 and mx["converged"] == 1
+    assert mx["n_products_mixed"] > 0
+    assert abs(mx["energy"] - fp["energy"]) / n < 1e-8
+    assert abs(mx["electrons"] - fp["electrons"]) < 1e-6
