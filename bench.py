@@ -225,8 +225,26 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="lnv512", choices=["lnv512", "batch", "serve", "mult216", "mult512"],
+                    help="lnv512: the plain FP64 512-atom solve (default); batch / serve: mixed-precision solves of "
+                         "many systems on concurrent slots vs the FP64 path one at a time; mult216 / mult512: single "
+                         "block products (216-atom DZP C=A.B; the products of one 512-atom LNV call)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3"])
+    ap.add_argument("--requests", type=int, default=32)
+    ap.add_argument("--nmin", type=int, default=64)
+    ap.add_argument("--nmax", type=int, default=1000)
+    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--rate", type=float, default=200.0)
     args = ap.parse_args()
     ws, rank, local = dist_env()
+    if args.workload in ("mult216", "mult512") and args.impl == "ours":
+        if rank == 0:
+            mult_main(args)
+        return
+    if args.workload != "lnv512" and args.impl == "ours":
+        if rank == 0:
+            serve_main(args)
+        return
     if args.impl == "reference":
         return reference_main(args, ws, rank)
     import torch
@@ -348,6 +366,163 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------------------
+# batched / served solves (the Batching-with-serving form)
+# ----------------------------------------------------------------------------
+SERVE_RANGES = (10.0, 12.0, 16.0, 10.0)   # S, H, L, T (bohr), as the 512-atom workload
+
+
+def request_set(n_req, nmin, nmax, seed):
+    """Seeded systems of the batched/served workloads: atom counts log-uniform in [nmin, nmax],
+    alternately clusters carved from the Si lattice and periodic supercells, 4x4 and 13x13 blocks
+    alternating in pairs, sigma = 0.1 bohr, per-request generator seed."""
+    from cq_b200 import inputs
+    rs = np.random.default_rng(seed)
+    out = []
+    for k in range(n_req):
+        n = int(round(np.exp(rs.uniform(np.log(nmin), np.log(nmax)))))
+        if k % 2 == 0:
+            c, cell = inputs.si_cluster(n, sigma=0.1, seed=1000 + k)
+        else:
+            m = int(np.clip(round((n / 8.0) ** (1.0 / 3.0)), 2, 6))
+            c, cell = inputs.diamond_si(m, sigma=0.1, seed=1000 + k)
+        nsf = 4 if (k // 2) % 2 == 0 else 13
+        ne = float(len(c)) if nsf == 4 else 2.0 * len(c)
+        out.append(dict(coords=c, cell=cell, nsf=nsf, ne=ne, seed=5000 + k, n=len(c)))
+    return out
+
+
+def run_server(cq_b200, reqs, n_slots, mixed, rate=None, seed=0):
+    """Submit the requests (all at once, or as a Poisson stream of `rate` per second) and wait for all."""
+    srv = cq_b200.Server(n_slots=n_slots, hbm_budget=int(0.8 * torch_total_mem()))
+    t_arr = np.zeros(len(reqs))
+    if rate:
+        t_arr = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, size=len(reqs)))
+    t0 = srv.now()
+    ids = []
+    for r, ta in zip(reqs, t_arr):
+        while srv.now() - t0 < ta:
+            time.sleep(min(0.002, max(0.0, ta - (srv.now() - t0))))
+        ids.append(srv.submit(r["coords"], r["cell"], r["nsf"], *SERVE_RANGES, r["ne"], seed=r["seed"], mixed=mixed,
+                              t_arrival=t0 + ta))
+    res = [srv.wait(i) for i in ids]
+    t1 = max(x["t_done"] for x in res)
+    srv.close()
+    return res, t1 - t0
+
+
+def torch_total_mem():
+    import torch
+    return torch.cuda.get_device_properties(0).total_memory
+
+
+def serve_main(args):
+    """Batched (all requests at t=0) or served (Poisson arrivals) density-matrix solves, mixed precision on
+    n_slots concurrent slots, against the plain FP64 path run one request at a time on the same set."""
+    import torch
+    import cq_b200
+    torch.cuda.set_device(0)
+    reqs = request_set(args.requests, args.nmin, args.nmax, seed=7)
+    rate = args.rate if args.workload == "serve" else None
+    warm = request_set(2, 64, 64, seed=99)
+    run_server(cq_b200, warm, 2, True)
+    with ClockSampler(0) as clk:
+        fp, t_fp = run_server(cq_b200, reqs, 1, False)
+        mx, t_mx = run_server(cq_b200, reqs, args.slots, True, rate=rate, seed=11)
+    bad = [r for r in fp + mx if r["status"] != 0]
+    err = max(abs(a["energy"] - b["energy"]) / a["n_atoms"] for a, b in zip(fp, mx))
+    lat = np.array([r["latency"] for r in mx]) * 1e3
+    atoms = sum(r["n"] for r in reqs)
+    flops_fp64 = sum(r["flops"] for r in fp)
+    line = {
+        "metric": "LNV solves/s (%s, mixed precision, %d slots)" % ("served" if rate else "batched", args.slots),
+        "value": len(reqs) / t_mx, "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
+        "dtype": "bf16x3+f64", "data": "synthetic (seeded Si clusters and supercells, S/H generators)",
+        "config": {"workload": "lnv_%s_si_mixed" % args.workload, "requests": len(reqs),
+                   "atoms": [args.nmin, args.nmax], "atoms_total": atoms, "blocks": "4x4 and 13x13",
+                   "ranges_bohr": dict(zip("SHLT", SERVE_RANGES)), "arrival_rate_per_s": rate,
+                   "slots": args.slots},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "fp64_path": {"value": len(reqs) / t_fp, "unit": "solves/s", "slots": 1,
+                      "latency_ms_p50": float(np.percentile([r["latency"] * 1e3 for r in fp], 50)),
+                      "block_mult_flops": flops_fp64},
+        "speedup_vs_fp64_path": t_fp / t_mx,
+        "max_energy_error_per_atom": err,
+        "failed": len(bad), "converged": sum(r["converged"] for r in mx),
+        "bytes_peak_max": max(r["bytes_peak"] for r in mx),
+        "clocks": clk.summary(),
+    }
+    emit(line)
+
+
+# ----------------------------------------------------------------------------
+# single products: config 1 (216-atom DZP mat_mult) and the products of one LNV call
+# ----------------------------------------------------------------------------
+def mult_main(args):
+    """Time block products on device-resident operands with CUDA events (L2 flushed before each launch).
+
+    mult216: C = A.B on a 216-atom Si supercell (3x3x3 cells, sigma 0.05), 13x13 blocks, A range 8,
+             B range 12, C range 20, entries uniform[-1,1] exp(-r/3).
+    lnv512:  the nine products of one LNV_matrix_multiply(M3, phi, E) call on the 512-atom SZ workload.
+    """
+    import torch
+    import cq_b200
+    from cq_b200 import inputs
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    prec = {"fp64": cq_b200.PREC_FP64, "fma": cq_b200.PREC_FP64_FMA, "bf16x3": cq_b200.PREC_BF16X3}[args.precision]
+    if args.workload == "mult216":
+        coords, cell = inputs.diamond_si(3, sigma=0.05, seed=1)
+        n = len(coords)
+        g = cq_b200.System(coords, cell, np.full(n, 13, np.int32), [8.0, 12.0, 20.0])
+        a = torch.from_numpy(inputs.random_blocks(g.blocklist(0, coords, cell), 1, inputs.TAG_RANDOM_A)).to(dev)
+        b = torch.from_numpy(inputs.random_blocks(g.blocklist(1, coords, cell), 1, inputs.TAG_RANDOM_B)).to(dev)
+        c = torch.zeros(g.length(2), dtype=torch.float64, device=dev)
+        prods = [("A.B->C", 1, 0, 1, 2, a, b, c)]
+        desc = "216-atom Si DZP (13x13), A 8 / B 12 / C 20 bohr"
+    else:
+        prob = build_problem(cq_b200)
+        g, ridx = prob["system"], prob["ridx"]
+        rs = np.random.default_rng(3)
+        mats = {k: torch.from_numpy(rs.uniform(-0.1, 0.1, g.length(ridx[k]))).to(dev) for k in
+                ("S", "H", "L", "LS", "LH", "LSL", "SLS")}
+        prods = []
+        for (t, x, y, z) in lnv_call_products():
+            prods.append(("%s_%s_%s/%d" % (x, y, z, t), t, ridx[x], ridx[y], ridx[z], mats[x], mats[y], mats[z]))
+        desc = "512-atom Si SZ (4x4), the nine products of one LNV call"
+    g.set_stream(stream.cuda_stream)
+    out = []
+    with ClockSampler(0) as clk:
+        for (name, t, ra, rb, rc, A, B, C) in prods:
+            triples, flops = g.product_work(t, ra, rb, rc)
+            for _ in range(args.warmup):
+                g.mat_mult(t, ra, rb, rc, A, B, C, precision=prec)
+            torch.cuda.synchronize()
+            ms = []
+            for _ in range(args.steps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                g.mat_mult(t, ra, rb, rc, A, B, C, precision=prec)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            m = float(np.median(ms))
+            nbytes = 8.0 * (g.length(ra) + g.length(rb) + g.length(rc))
+            out.append({"product": name, "triples": triples, "flops": flops, "ms": m,
+                        "tflops": flops / (m / 1e3) / 1e12, "gbs_algorithmic": nbytes / (m / 1e3) / 1e9})
+    tot_fl = sum(o["flops"] for o in out)
+    tot_ms = sum(o["ms"] for o in out)
+    emit({"metric": "block-mult TFLOP/s (%s)" % args.precision, "value": tot_fl / (tot_ms / 1e3) / 1e12,
+          "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+          "dtype": {"fp64": "f64", "fma": "f64", "bf16x3": "bf16x3"}[args.precision],
+          "data": "synthetic", "config": {"workload": args.workload, "system": desc,
+                                          "l2": "flushed (256 MB write) before every timed launch"},
+          "products": out, "clocks": clk.summary()})
 
 
 def solve_host_pinned(solver, pinS, pinH, pinL, pinK):

@@ -38,7 +38,8 @@ class LNVResult(ctypes.Structure):
     """cq_lnv_result (include/cq_b200.h)."""
     _fields_ = [("energy", c_double), ("electrons", c_double), ("residual", c_double), ("invs_omega", c_double),
                 ("mcw_sweeps", c_int), ("early_iters", c_int), ("late_iters", c_int), ("ne_corrections", c_int),
-                ("inflexions", c_int), ("converged", c_int), ("n_products", c_int64), ("flops", c_int64),
+                ("inflexions", c_int), ("converged", c_int), ("outer_iters", c_int), ("n_products", c_int64),
+                ("flops", c_int64),
                 ("n_products_mixed", c_int64), ("flops_mixed", c_int64)]
 
     def as_dict(self):
@@ -114,6 +115,7 @@ def lib():
         "cq_lnv_get": [c_void_p, ctypes.c_char_p, c_void_p, c_int64, c_int],
         "cq_lnv_put": [c_void_p, ctypes.c_char_p, c_void_p, c_int],
         "cq_lnv_solve_host": [c_void_p, P(c_double), P(c_double), P(c_double), P(c_double), P(LNVResult)],
+        "cq_lnv_reduction_log": [c_void_p, c_int, P(c_double), c_int64, P(c_int64)],
     }
     for name, args in lnv_sigs.items():
         f = getattr(L, name)
@@ -367,6 +369,13 @@ class LNV:
     def put(self, name, arr):
         arr = np.ascontiguousarray(arr, np.float64)
         check(lib().cq_lnv_put(self._h, name.encode(), arr.ctypes.data_as(c_void_p), 0))
+
+    def reduction_log(self, enable=True, cap=1 << 20):
+        """Trace values recorded since the last call, in call order; then clear the log and set recording."""
+        out = np.zeros(cap)
+        n = c_int64()
+        check(lib().cq_lnv_reduction_log(self._h, int(bool(enable)), _dp(out), cap, ctypes.byref(n)))
+        return out[:min(n.value, cap)]
 
     def solve_host(self, S, H, want_L=False, want_K=False):
         S = np.ascontiguousarray(S, np.float64); H = np.ascontiguousarray(H, np.float64)

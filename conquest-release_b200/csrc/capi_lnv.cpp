@@ -1,4 +1,5 @@
 // C ABI of the LNV / McWeeny solver (declarations in include/cq_b200.h).
+#include <algorithm>
 #include <cstring>
 #include <functional>
 #include <string>
@@ -26,6 +27,7 @@ static void fill_result(const LNVStats& st, cq_lnv_result* r) {
   r->ne_corrections = st.ne_corrections;
   r->inflexions = st.inflexions;
   r->converged = st.converged;
+  r->outer_iters = st.outer_iters;
   r->n_products = st.n_products;
   r->flops = st.flops;
   r->n_products_mixed = st.n_products_mixed;
@@ -59,7 +61,7 @@ int cq_lnv_params_default(cq_lnv_params* p) {
   p->invs_delta_tol = 1.0e-4;
   p->invs_tol = 1.0e-2;
   p->exact = 1;
-  p->max_outer = 1000;
+  p->max_outer = 40;
   p->mixed = 0;
   p->mixed_tolerance = 1.0e-5;
   return CQ_OK;
@@ -169,6 +171,17 @@ int cq_lnv_solve_host(cq_lnv* s, const double* S, const double* H, double* L_out
     if (K_out) CQ_CUDA(cudaMemcpyAsync(K_out, L.K.p, sizeof(double) * L.K.n, cudaMemcpyDeviceToHost, L.S.stream));
     CQ_CUDA(cudaStreamSynchronize(L.S.stream));
     fill_result(L.stats, res);
+  });
+}
+
+int cq_lnv_reduction_log(cq_lnv* s, int enable, double* out, int64_t cap, int64_t* n) {
+  return guarded_call([&] {
+    CQ_CHECK(s, CQ_ERR_ARG, "null argument");
+    LNVSolver& L = *s->solver;
+    if (n) *n = (int64_t)L.rlog.size();
+    if (out) std::memcpy(out, L.rlog.data(), sizeof(double) * std::min<int64_t>(cap, (int64_t)L.rlog.size()));
+    L.rlog_on = enable != 0;
+    L.rlog.clear();
   });
 }
 

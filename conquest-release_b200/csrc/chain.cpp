@@ -130,9 +130,16 @@ void LNVSolver::transpose(const DMat& A, DMat& AT) { dev_transpose(S, R[A.rng], 
 double LNVSolver::ptrace(const DMat& A, const DMat& B) {
   CQ_CHECK(A.rng == B.rng, CQ_ERR_STATE, "matrix_product_trace needs equal ranges");
   stats.n_reductions++;
-  return dev_dot(S, A.p, B.p, A.n);
+  double v = dev_dot(S, A.p, B.p, A.n);
+  if (rlog_on) rlog.push_back(v);
+  return v;
 }
-double LNVSolver::trace(const DMat& A) { stats.n_reductions++; return dev_trace(S, R[A.rng], A.p); }
+double LNVSolver::trace(const DMat& A) {
+  stats.n_reductions++;
+  double v = dev_trace(S, R[A.rng], A.p);
+  if (rlog_on) rlog.push_back(v);
+  return v;
+}
 void LNVSolver::copy(DMat& dst, const DMat& src) { dev_copy(S, dst.p, src.p, src.n); }
 
 void LNVSolver::set_identity_onsite(DMat& A) {
@@ -642,7 +649,10 @@ void LNVSolver::find_min_dm(bool resetL) {
   transpose(T, Ttran);
   int ndone = 0, niter = 0, outer = 0;
   while (!done) {
-    CQ_CHECK(++outer <= prm.max_outer, CQ_ERR_NOT_CONVERGED, "FindMinDM: no convergence within the outer-iteration limit");
+    // the reference loops until done; a problem whose residual stalls above the tolerance stops
+    // here after max_outer passes, reported as not converged
+    if (++outer > prm.max_outer) break;
+    stats.outer_iters++;
     if (resetL || inflex) {
       init_mcw();
       delta_e = mcw_min(prm.n_L_iterations);
@@ -662,7 +672,7 @@ void LNVSolver::find_min_dm(bool resetL) {
   lnv(true, false, true, true, nullptr, &phi, &el, &en);
   stats.energy = 2.0 * en;
   stats.electrons = 2.0 * el;
-  stats.converged = 1;
+  stats.converged = done ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------

@@ -35,6 +35,7 @@ bool sym_inverse_bk(double* A, int n);
 struct LNVStats {
   int64_t n_products = 0, flops = 0, n_reductions = 0, n_lnv = 0, n_products_mixed = 0, flops_mixed = 0;
   int mcw_sweeps = 0, early_iters = 0, late_iters = 0, ne_corrections = 0, inflexions = 0, converged = 0;
+  int outer_iters = 0;
   double energy = 0, electrons = 0, last_energy = 0, last_residual = 0, invs_omega = 0;
   double mubar = 0, lambda = 0, hmin = 0, hmax = 0;
 };
@@ -57,6 +58,8 @@ class LNVSolver {
   int ni_in_cell;
   double delta_e = 0.0;  // `save` variable of FindMinDM
   LNVStats stats;
+  std::vector<double> rlog;   // every trace / product-trace value in call order, when rlog_on
+  bool rlog_on = false;
   DMat Smat, Hmat, L, T, Ttran, LS, SL, K, phi;
 
   DMat temp(int rng);

