@@ -230,6 +230,7 @@ def main():
                          "many systems on concurrent slots vs the FP64 path one at a time; mult216 / mult512: single "
                          "block products (216-atom DZP C=A.B; the products of one 512-atom LNV call)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3"])
+    ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (0, 1, 2)")
     ap.add_argument("--requests", type=int, default=32)
     ap.add_argument("--nmin", type=int, default=64)
     ap.add_argument("--nmax", type=int, default=1000)
@@ -257,7 +258,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     prob = build_problem(cq_b200)
     system, solver = prob["system"], prob["solver"]
-    stream = torch.cuda.current_stream()
+    if args.variant is not None:
+        system.set_mult_variant(args.variant)
+    # a dedicated stream: the library enqueues on it and the CUDA events are recorded on it (torch's
+    # default stream handle is 0, which the library reads as "its own stream")
+    stream = torch.cuda.Stream(device=torch.device("cuda", local))
+    torch.cuda.set_stream(stream)
     system.set_stream(stream.cuda_stream)
     dev = torch.device("cuda", local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # 256 MB > 126 MB L2
@@ -372,6 +378,9 @@ def main():
 # batched / served solves (the Batching-with-serving form)
 # ----------------------------------------------------------------------------
 SERVE_RANGES = (10.0, 12.0, 16.0, 10.0)   # S, H, L, T (bohr), as the 512-atom workload
+# residual at which both arms stop: at the default 1e-7 two FP64 solves of one problem from different
+# starting points differ by ~1e-7 Ha/atom, so the 1e-8 Ha/atom comparison needs a tighter stop
+SERVE_TOL = 1e-9
 
 
 def request_set(n_req, nmin, nmax, seed):
@@ -396,7 +405,7 @@ def request_set(n_req, nmin, nmax, seed):
 
 def run_server(cq_b200, reqs, n_slots, mixed, rate=None, seed=0):
     """Submit the requests (all at once, or as a Poisson stream of `rate` per second) and wait for all."""
-    srv = cq_b200.Server(n_slots=n_slots, hbm_budget=int(0.8 * torch_total_mem()))
+    srv = cq_b200.Server(n_slots=n_slots, hbm_budget=int(0.8 * torch_total_mem()), tolerance=SERVE_TOL)
     t_arr = np.zeros(len(reqs))
     if rate:
         t_arr = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, size=len(reqs)))
@@ -443,7 +452,7 @@ def serve_main(args):
         "config": {"workload": "lnv_%s_si_mixed" % args.workload, "requests": len(reqs),
                    "atoms": [args.nmin, args.nmax], "atoms_total": atoms, "blocks": "4x4 and 13x13",
                    "ranges_bohr": dict(zip("SHLT", SERVE_RANGES)), "arrival_rate_per_s": rate,
-                   "slots": args.slots},
+                   "slots": args.slots, "tolerance": SERVE_TOL},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "fp64_path": {"value": len(reqs) / t_fp, "unit": "solves/s", "slots": 1,
                       "latency_ms_p50": float(np.percentile([r["latency"] * 1e3 for r in fp], 50)),
@@ -472,7 +481,8 @@ def mult_main(args):
     from cq_b200 import inputs
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream(device=dev)      # the library's stream, where the events are recorded
+    torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     prec = {"fp64": cq_b200.PREC_FP64, "fma": cq_b200.PREC_FP64_FMA, "bf16x3": cq_b200.PREC_BF16X3}[args.precision]
     if args.workload == "mult216":
@@ -495,6 +505,8 @@ def mult_main(args):
             prods.append(("%s_%s_%s/%d" % (x, y, z, t), t, ridx[x], ridx[y], ridx[z], mats[x], mats[y], mats[z]))
         desc = "512-atom Si SZ (4x4), the nine products of one LNV call"
     g.set_stream(stream.cuda_stream)
+    if args.variant is not None:
+        g.set_mult_variant(args.variant)
     out = []
     with ClockSampler(0) as clk:
         for (name, t, ra, rb, rc, A, B, C) in prods:
@@ -520,7 +532,7 @@ def mult_main(args):
     emit({"metric": "block-mult TFLOP/s (%s)" % args.precision, "value": tot_fl / (tot_ms / 1e3) / 1e12,
           "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
           "dtype": {"fp64": "f64", "fma": "f64", "bf16x3": "bf16x3"}[args.precision],
-          "data": "synthetic", "config": {"workload": args.workload, "system": desc,
+          "data": "synthetic", "config": {"workload": args.workload, "system": desc, "variant": args.variant,
                                           "l2": "flushed (256 MB write) before every timed launch"},
           "products": out, "clocks": clk.summary()})
 

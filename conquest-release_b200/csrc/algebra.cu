@@ -18,7 +18,7 @@ namespace cqb {
 namespace {
 
 constexpr int kT = 256;
-constexpr int kRedBlocks = 1184;   // 148 SMs x 8: fixed so the reduction order never changes
+constexpr int kRedBlocks = 1184;   // 148 SMs x 8: the largest grid of the exact sums
 
 int grid_for(int64_t n) {
   int64_t b = (n + kT - 1) / kT;
@@ -72,6 +72,7 @@ __global__ void k_transpose(int nnz, const int* __restrict__ dest, const int64_t
 // Terms below 2^(emax-150) are truncated toward zero (relative effect < n 2^-150).
 // ---------------------------------------------------------------------------
 constexpr int kAccFrac = 150;   // fraction bits kept below the largest term's exponent
+constexpr int kSumSlots = 32;   // exact sums fetched together by dev_dots
 constexpr int kEBias = 2048;    // exponent bias of the pass-1 maximum (frexp exponents lie in [-1073, 1024])
 
 struct Acc192 { uint64_t w[3]; };
@@ -306,14 +307,33 @@ static double exact_sum_value(const uint64_t r[4]) {
   return acc192_to_double(r, eb - kEBias - kAccFrac);
 }
 
+// Scratch of the exact sums: the block partials of the sum being computed (the three passes of
+// one sum run back to back on the stream, so consecutive sums share them), then one 4-word
+// result per slot; two flag words per slot.
+static void acc_scratch(System& S) {
+  if (S.acc_part.n < (size_t)(3 * kRedBlocks + 4 * kSumSlots)) S.acc_part.alloc(3 * kRedBlocks + 4 * kSumSlots, S.stream);
+  if (S.acc_flags.n < (size_t)(2 * kSumSlots)) S.acc_flags.alloc(2 * kSumSlots, S.stream);
+}
+
 static double exact_sum(System& S, const double* x, const double* y, int64_t n) {
-  if (S.acc_part.n < (size_t)(3 * kRedBlocks + 4)) S.acc_part.alloc(3 * kRedBlocks + 4, S.stream);
-  if (S.acc_flags.n < 2) S.acc_flags.alloc(2, S.stream);
+  acc_scratch(S);
   exact_sum_enqueue(S, x, y, n, S.acc_flags.p, S.acc_part.p, S.acc_part.p + 3 * kRedBlocks);
   uint64_t w[4];
   CQ_CUDA(cudaMemcpyAsync(w, S.acc_part.p + 3 * kRedBlocks, sizeof(w), cudaMemcpyDeviceToHost, S.stream));
   host_wait(S);
   return exact_sum_value(w);
+}
+
+void dev_dots(System& S, int count, const double* const* x, const double* const* y, const int64_t* n, double* out) {
+  CQ_CHECK(count >= 0 && count <= kSumSlots, CQ_ERR_ARG, "too many sums in one batch");
+  if (count == 0) return;
+  acc_scratch(S);
+  uint64_t* res = S.acc_part.p + 3 * kRedBlocks;
+  for (int k = 0; k < count; ++k) exact_sum_enqueue(S, x[k], y[k], n[k], S.acc_flags.p + 2 * k, S.acc_part.p, res + 4 * k);
+  std::vector<uint64_t> w(4 * (size_t)count);
+  CQ_CUDA(cudaMemcpyAsync(w.data(), res, sizeof(uint64_t) * w.size(), cudaMemcpyDeviceToHost, S.stream));
+  host_wait(S);
+  for (int k = 0; k < count; ++k) out[k] = exact_sum_value(&w[4 * k]);
 }
 
 double dev_dot(System& S, const double* x, const double* y, int64_t n) { return exact_sum(S, x, y, n); }

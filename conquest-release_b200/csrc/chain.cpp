@@ -134,6 +134,22 @@ double LNVSolver::ptrace(const DMat& A, const DMat& B) {
   if (rlog_on) rlog.push_back(v);
   return v;
 }
+// Several matrix_product_trace values computed back to back and read with one host wait; the
+// values (and the reduction log) are those of the same ptrace calls in this order.
+void LNVSolver::ptraces(std::initializer_list<std::pair<const DMat*, const DMat*>> ops, double* out) {
+  const double* xs[32];
+  const double* ys[32];
+  int64_t ns[32];
+  int k = 0;
+  for (auto& o : ops) {
+    CQ_CHECK(o.first->rng == o.second->rng, CQ_ERR_STATE, "matrix_product_trace needs equal ranges");
+    xs[k] = o.first->p; ys[k] = o.second->p; ns[k] = o.first->n;
+    ++k;
+  }
+  stats.n_reductions += k;
+  dev_dots(S, k, xs, ys, ns, out);
+  if (rlog_on) rlog.insert(rlog.end(), out, out + k);
+}
 double LNVSolver::trace(const DMat& A) {
   stats.n_reductions++;
   double v = dev_trace(S, R[A.rng], A.p);
@@ -210,18 +226,26 @@ void LNVSolver::lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* p
     msum(0.0, K, 3.0, LSL);
     msum(1.0, K, -2.0, LSLSL);
   }
-  if (doE) *energy = ptrace(Hmat, K);
   if (doM3) {
     msum(0.0, *M3, 3.0, HLS);
     msum(1.0, *M3, 3.0, SLH);
     msum(1.0, *M3, -1.0, Bm);
     msum(1.0, *M3, -1.0, Cm);
   }
+  // Tr(HK), Tr(L SLS), Tr(L SLSLS): enqueued back to back (before phi is overwritten) and read
+  // together; the reference computes them in this order (mult_module.f90:1700-1800)
+  double t[3];
+  if (dophi) msum(0.0, *phim, 1.0, SLS);
+  if (doE && dophi) {
+    ptraces({{&Hmat, &K}, {&L, phim}, {&L, &SLSLS}}, t);
+  } else if (doE) {
+    ptraces({{&Hmat, &K}}, t);
+  } else if (dophi) {
+    ptraces({{&L, phim}, {&L, &SLSLS}}, t + 1);
+  }
+  if (doE) *energy = t[0];
   if (dophi) {
-    msum(0.0, *phim, 1.0, SLS);
-    double e1 = ptrace(L, *phim);
-    double e2 = ptrace(L, SLSLS);
-    *electrons = 3.0 * e1 - 2.0 * e2;
+    *electrons = 3.0 * t[1] - 2.0 * t[2];
     msum(6.0, *phim, -6.0, SLSLS);
   }
   stats.n_lnv++;
@@ -344,10 +368,11 @@ void LNVSolver::mcw_mm_nonds(DMat& RhoNew, double& energy, double& c) {
   product(LSL, LS, LSLSL, HLS_LS_L);
   msum(0.0, top, 1.0, LSL);
   msum(1.0, top, -1.0, LSLSL);
-  double c1 = ptrace(Smat, top);
   msum(0.0, bottom, 1.0, L);
   msum(1.0, bottom, -1.0, LSL);
-  double c2 = ptrace(Smat, bottom);
+  double cc[2];
+  ptraces({{&Smat, &top}, {&Smat, &bottom}}, cc);
+  const double c1 = cc[0], c2 = cc[1];
   CQ_CHECK(std::fabs(c2) > 1e-15, CQ_ERR_NOT_CONVERGED, "McW_matrix_multiply: c2 is near zero");
   double cn = c1 / c2;
   c = cn;
@@ -467,8 +492,10 @@ bool LNVSolver::line_min_L(DMat& M3, DMat& D, DMat& mtemp, DMat& SM3, double ene
   double el, e1;
   lnv(true, true, false, true, &M3, nullptr, &el, &e1);
   double energy_1 = 2.0 * e1;
-  double g1 = 2.0 * ptrace(D, M3);
-  double igcross = 2.0 * ptrace(SM3, M3);
+  double gg[2];
+  ptraces({{&D, &M3}, {&SM3, &M3}}, gg);
+  double g1 = 2.0 * gg[0];
+  double igcross = 2.0 * gg[1];
   tmt(M3, SM3, mtemp, T);
   double ig1 = 2.0 * ptrace(SM3, M3);
   double ig1_step = ig1;
@@ -492,8 +519,10 @@ bool LNVSolver::line_min_L(DMat& M3, DMat& D, DMat& mtemp, DMat& SM3, double ene
     zeta = (interpG - ig1) / (ig0 - ig1);
   } else {
     tmt(M3, SM3, mtemp, T);
-    ig1 = 2.0 * ptrace(SM3, M3);
-    igcross = 2.0 * ptrace(SM3, M3old);
+    double ii[2];
+    ptraces({{&SM3, &M3}, {&SM3, &M3old}}, ii);
+    ig1 = 2.0 * ii[0];
+    igcross = 2.0 * ii[1];
     lamG = step / truestep;
     interpG = ig0 * (1 - lamG) * (1 - lamG) + ig1 * lamG * lamG + 2.0 * igcross * lamG * (1 - lamG);
     zeta = (interpG - ig1_step) / (ig0 - ig1_step);
@@ -503,15 +532,17 @@ bool LNVSolver::line_min_L(DMat& M3, DMat& D, DMat& mtemp, DMat& SM3, double ene
 
 void LNVSolver::project_search(DMat& search, DMat& SM3, DMat& Sphi, DMat& mtemp) {
   tmt(phi, Sphi, mtemp, T);
-  double e_dot_n = ptrace(SM3, phi);
-  double n_dot_n = ptrace(Sphi, phi);
+  double d[2];
+  ptraces({{&SM3, &phi}, {&Sphi, &phi}}, d);
+  const double e_dot_n = d[0], n_dot_n = d[1];
   if (std::fabs(n_dot_n) > 1.0e-8) msum(1.0, search, e_dot_n / n_dot_n, Sphi);
 }
 
 void LNVSolver::project_gradient(DMat& M3, DMat& SM3, DMat& Sphi, DMat& mtemp) {
   tmt(phi, Sphi, mtemp, T);
-  double e_dot_n = ptrace(SM3, phi), n_dot_n = ptrace(Sphi, phi);
-  double et = 2.0 * e_dot_n, nt = 2.0 * n_dot_n;
+  double d[2];
+  ptraces({{&SM3, &phi}, {&Sphi, &phi}}, d);
+  double et = 2.0 * d[0], nt = 2.0 * d[1];
   if (std::fabs(nt) > 1.0e-8) {
     double f = et / nt;
     msum(1.0, SM3, -f, Sphi);
@@ -583,7 +614,9 @@ int LNVSolver::late_dm(int ndone, bool& done, double& deltaE) {
   tmt(M3, SM3, mtemp, T);
   if (prm.vary_mu) {
     tmt(phi, Sphi, mtemp, T);
-    double e_dot_n = ptrace(SM3, phi), n_dot_n = ptrace(Sphi, phi);
+    double d[2];
+    ptraces({{&SM3, &phi}, {&Sphi, &phi}}, d);
+    const double e_dot_n = d[0], n_dot_n = d[1];
     if (std::fabs(n_dot_n) > 1.0e-8) {
       double f = e_dot_n / n_dot_n;
       msum(1.0, SM3, -f, Sphi);
@@ -615,8 +648,22 @@ int LNVSolver::late_dm(int ndone, bool& done, double& deltaE) {
     msum(0.0, Gst[npmod - 1], -1.0, M3);
     msum(0.0, Lst[npmod - 1], 1.0, L);
     std::fill(Aij.begin(), Aij.end(), 0.0);
-    for (int i = 0; i < pul_mx; ++i)
-      for (int j = 0; j < pul_mx; ++j) Aij[j + npul * i] = 2.0 * ptrace(Gst[j], SGst[i]);
+    {
+      // the pul_mx^2 traces Tr(G_j SG_i), in the reference's loop order, read with one wait
+      const double* xs[32];
+      const double* ys[32];
+      int64_t ns[32];
+      double v[32];
+      int k = 0;
+      for (int i = 0; i < pul_mx; ++i)
+        for (int j = 0; j < pul_mx; ++j) { xs[k] = Gst[j].p; ys[k] = SGst[i].p; ns[k] = Gst[j].n; ++k; }
+      stats.n_reductions += k;
+      dev_dots(S, k, xs, ys, ns, v);
+      if (rlog_on) rlog.insert(rlog.end(), v, v + k);
+      k = 0;
+      for (int i = 0; i < pul_mx; ++i)
+        for (int j = 0; j < pul_mx; ++j) Aij[j + npul * i] = 2.0 * v[k++];
+    }
     do_pulay(npmod, Aij.data(), pul_mx, npul, alph.data());
     scale(0.0, L);
     for (int i = 0; i < pul_mx; ++i) msum(1.0, L, alph[i], Lst[i]);

@@ -1,5 +1,7 @@
 // LNV / McWeeny solver state (see chain.cpp).
 #pragma once
+#include <initializer_list>
+#include <utility>
 #include <vector>
 
 #include "cq_internal.hpp"
@@ -86,6 +88,7 @@ class LNVSolver {
   void scale(double alpha, DMat& A);
   void transpose(const DMat& A, DMat& AT);
   double ptrace(const DMat& A, const DMat& B);
+  void ptraces(std::initializer_list<std::pair<const DMat*, const DMat*>> ops, double* out);
   double trace(const DMat& A);
   void copy(DMat& dst, const DMat& src);
   void set_identity_onsite(DMat& A);

@@ -201,6 +201,8 @@ struct ProductPlan {
   int64_t flops = 0;              // 2 * sum nd_i nd_j nd_k over the triples
   DevBuf<int64_t> ptr;            // [n_out_blocks+1]
   DevBuf<int2> pairs;             // [n_pairs] (x block, b block)
+  int n_tiles = 0;                // row tiles of the staged 4x4 kernel: (q0, q1, x row first, x row end)
+  DevBuf<int4> tiles;
 };
 
 // Split-precision tensor-core product: pair lists sorted by the first operand block,
@@ -257,7 +259,8 @@ struct System {
   DevBuf<int> diag_off;           // first onsite-diagonal slot of each primary atom
   DevBuf<double> diag_buf;        // gathered onsite diagonal (exact trace)
   int64_t launches = 0;           // kernels launched by this system (all kinds)
-  int mult_variant = 1;           // 4x4 FP64 product kernel: 0 = one lane per element, 1 = one thread per block
+  int mult_variant = 1;           // 4x4 FP64 product kernel: 0 = one lane per element, 1 = one thread per block,
+                                  // 2 = one thread per block with the operand row staged in shared memory
   bool blocking_sync = false;     // host waits sleep on a blocking-sync event instead of spinning
   cudaEvent_t sync_ev = nullptr;
   ProductProfile prof;
@@ -296,6 +299,9 @@ void dev_copy(System& S, double* dst, const double* src, int64_t n);
 void dev_matrix_add(System& S, int ra, double* a, double alpha, int rb, const double* b, double beta);
 void dev_transpose(System& S, int r, const double* a, double* at);
 double dev_dot(System& S, const double* x, const double* y, int64_t n);
+// up to 32 exact dot products (y[k] may be null: plain sums), computed back to back and read
+// with one host synchronisation
+void dev_dots(System& S, int count, const double* const* x, const double* const* y, const int64_t* n, double* out);
 double dev_trace(System& S, int r, const double* a);
 void dev_h_limits(System& S, int r, const double* h, double* hmin, double* hmax);
 

@@ -178,6 +178,77 @@ __global__ void __launch_bounds__(128) k_mult_nd4_tpb(MultArgs M) {
   for (int v = 0; v < 8; ++v) O2[v] = make_double2(acc[2 * v], acc[2 * v + 1]);
 }
 
+// 4 x 4 blocks, one thread per output block, the first operand's row staged in shared memory.
+// A CTA owns up to 128 consecutive output blocks of one row i; every pair of those blocks reads
+// its first operand from row i of that operand (A_ik for type 1, c_ij for type 2), so the row
+// is copied into shared memory in chunks of CHUNK blocks with coalesced 16-byte loads, and each
+// thread walks its pair list in order, taking the pairs whose operand lies in the current chunk
+// (a pair list that goes back to an earlier chunk reads that block from global memory, so the
+// order of the terms is never changed).  Only the B blocks come from L2 per pair.
+template <int TYPE, bool EXACT, int CHUNK>
+__global__ void __launch_bounds__(128) k_mult_nd4_rows(MultArgs M, const int4* __restrict__ tiles) {
+  __shared__ double2 xs[CHUNK * 8];
+  const int4 d = tiles[blockIdx.x];           // output blocks [d.x, d.y), operand row blocks [d.z, d.w)
+  const int q = d.x + (int)threadIdx.x;
+  int64_t t = 0, tend = 0;
+  if (q < d.y) { t = M.ptr[q]; tend = M.ptr[q + 1]; }
+  double acc[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+  const double2* X2g = reinterpret_cast<const double2*>(M.x);
+  const double2* B2g = reinterpret_cast<const double2*>(M.b);
+  for (int c0 = d.z; c0 < d.w; c0 += CHUNK) {
+    const int c1 = min(c0 + CHUNK, d.w);
+    __syncthreads();
+    for (int v = threadIdx.x; v < (c1 - c0) * 8; v += blockDim.x) xs[v] = __ldg(X2g + (int64_t)c0 * 8 + v);
+    __syncthreads();
+    while (t < tend) {
+      const int2 pr = M.pairs[t];
+      if (pr.x >= c1) break;
+      double x[16], b[16];
+      const double2* B2 = B2g + (int64_t)pr.y * 8;
+      if (pr.x >= c0) {
+        const double2* X2 = xs + (pr.x - c0) * 8;
+#pragma unroll
+        for (int v = 0; v < 8; ++v) { double2 xv = X2[v]; x[2 * v] = xv.x; x[2 * v + 1] = xv.y; }
+      } else {
+        const double2* X2 = X2g + (int64_t)pr.x * 8;
+#pragma unroll
+        for (int v = 0; v < 8; ++v) { double2 xv = __ldg(X2 + v); x[2 * v] = xv.x; x[2 * v + 1] = xv.y; }
+      }
+#pragma unroll
+      for (int v = 0; v < 8; ++v) { double2 bv = __ldg(B2 + v); b[2 * v] = bv.x; b[2 * v + 1] = bv.y; }
+      if (TYPE == 1) {
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+          for (int n1 = 0; n1 < 4; ++n1) {
+            double a = acc[n1 + 4 * m];
+#pragma unroll
+            for (int n3 = 0; n3 < 4; ++n3) a = madd<EXACT>(a, x[n1 + 4 * n3], b[n3 + 4 * m]);
+            acc[n1 + 4 * m] = a;
+          }
+      } else {
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+          for (int n1 = 0; n1 < 4; ++n1) {
+            double a = acc[n1 + 4 * m];
+#pragma unroll
+            for (int n2 = 0; n2 < 4; ++n2) a = madd<EXACT>(a, x[n1 + 4 * n2], b[m + 4 * n2]);
+            acc[n1 + 4 * m] = a;
+          }
+      }
+      ++t;
+    }
+  }
+  if (q < d.y) {
+    double2* O2 = reinterpret_cast<double2*>(M.out + 16 * (int64_t)q);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) O2[v] = make_double2(acc[2 * v], acc[2 * v + 1]);
+  }
+}
+
 // One drop-in m_kern_max (type 1) / m_kern_min (type 2) call: output blocks with explicit
 // offsets, accumulated in place in the layouts mat_mult passes (type 1 reads the local
 // transpose a(n3 + nd3*n1); type 2 accumulates into it).  One warp per output block.
@@ -247,7 +318,25 @@ void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, doub
   S.launches++;
   // the 4 x 4 path reads B with 16-byte vector loads: require 16-byte aligned operands
   bool aligned = ((uintptr_t)b % 16 == 0) && ((uintptr_t)M.x % 16 == 0) && ((uintptr_t)M.out % 16 == 0);
-  if (S.uniform_nsf == 4 && aligned && S.mult_variant == 1) {
+  if (S.uniform_nsf == 4 && aligned && S.mult_variant == 2) {
+    constexpr int kChunk = 256;                 // 32 KiB of operand blocks per chunk
+    if (P.n_tiles == 0) {
+      // tiles: up to 128 output blocks of one row, with that row's range of operand blocks
+      std::vector<int4> tl;
+      for (int i = 0; i < S.geo.n_prim; ++i)
+        for (int q0 = O.h_row_ptr[i]; q0 < O.h_row_ptr[i + 1]; q0 += 128)
+          tl.push_back(make_int4(q0, std::min(q0 + 128, O.h_row_ptr[i + 1]), X.h_row_ptr[i], X.h_row_ptr[i + 1]));
+      P.tiles.upload(tl, st);
+      P.n_tiles = (int)tl.size();
+    }
+    if (P.mult_type == 1) {
+      if (exact) k_mult_nd4_rows<1, true, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
+      else k_mult_nd4_rows<1, false, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
+    } else {
+      if (exact) k_mult_nd4_rows<2, true, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
+      else k_mult_nd4_rows<2, false, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
+    }
+  } else if (S.uniform_nsf == 4 && aligned && S.mult_variant == 1) {
     const int T1 = 128;
     int grid = (M.n_out + T1 - 1) / T1;
     if (P.mult_type == 1) {

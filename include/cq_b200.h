@@ -170,7 +170,8 @@ int cq_launch_count(cq_system* sys, int64_t* count);
 int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out);
 
 /* Tuning options.  CQ_OPT_MULT_VARIANT: FP64 4x4 product kernel, 0 = one lane per output
- * element, 1 = one thread per output block (default).  Both give identical results.
+ * element, 1 = one thread per output block (default), 2 = one thread per output block with the
+ * first operand's row staged in shared memory.  All give identical results.
  * CQ_OPT_BLOCKING_SYNC: 1 = the host thread sleeps on a blocking-sync event whenever the
  * solver waits for a scalar from the device (many concurrent solvers per host core), 0 = it
  * spins in cudaStreamSynchronize (default, lowest latency for one solver). */
