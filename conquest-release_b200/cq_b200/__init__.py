@@ -511,3 +511,25 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+NOALLOC_MAX_SUMS = 8   # CQ_NOALLOC_MAX_SUMS
+
+
+def exact_dots_noalloc(xs, ys=None, stream=None):
+    """cq_exact_dots_noalloc: exact dot products (plain sums where ys[k] is None) of device arrays,
+    with the scratch in a static device array, for callers that cannot allocate device memory.
+    Calls that overlap on the GPU share that scratch and must be serialised by the caller."""
+    L = lib()
+    f = L.cq_exact_dots_noalloc
+    f.argtypes = [c_int, P(c_void_p), P(c_void_p), P(c_int64), c_void_p, P(c_double)]
+    f.restype = c_int
+    k = len(xs)
+    xp = (c_void_p * max(k, 1))(*[_ptr(x).value for x in xs])
+    yp = None
+    if ys is not None:
+        yp = (c_void_p * max(k, 1))(*[(_ptr(y).value if y is not None else None) for y in ys])
+    ns = (c_int64 * max(k, 1))(*[int(x.numel()) for x in xs])
+    out = (c_double * max(k, 1))()
+    check(f(k, xp, yp, ns, c_void_p(stream) if stream else None, out))
+    return [out[i] for i in range(k)]

@@ -9,6 +9,8 @@
 // the reductions are two-level with a fixed grid, so results are identical
 // from run to run.
 #include <climits>
+#include <functional>
+#include <mutex>
 #include <cmath>
 #include <limits>
 
@@ -369,4 +371,75 @@ void dev_h_limits(System& S, int r, const double* h, double* hmin, double* hmax)
   *hmax = o[1];
 }
 
+// ---------------------------------------------------------------------------
+// Exact dot products without any device allocation (cq_exact_dots_noalloc).
+//
+// Some callers cannot allocate device memory at the moment they need a trace: a Fortran/MPI
+// host that has given the whole device to its own memory pool, or a latency-critical loop that
+// must not take the device-wide synchronisation cudaMalloc and cudaFree can imply.  This entry
+// point runs the same three kernels as the library's traces, with their scratch (block
+// partials, results and flags) in one static device array instead of library-allocated memory.
+// Every call uses that same array, so calls that overlap on the GPU (from two streams or two
+// threads) race on it.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kNoAllocSums = CQ_NOALLOC_MAX_SUMS;
+// words: block partials of one sum | 4-word result per sum | 2 int flags per sum (one word)
+constexpr int kNoAllocWords = 3 * kRedBlocks + 4 * kNoAllocSums + kNoAllocSums;
+static __device__ __align__(256) uint64_t g_noalloc_scratch[kNoAllocWords];   // 28.7 KiB per device
+
+std::mutex g_noalloc_mu;
+uint64_t* g_noalloc_addr[64] = {};   // device address of g_noalloc_scratch, per device ordinal
+
+// Device address of the static scratch on the current device, looked up once per device (the
+// host-side name of the array is not a device address).
+uint64_t* noalloc_scratch() {
+  int dev = 0;
+  CQ_CUDA(cudaGetDevice(&dev));
+  CQ_CHECK(dev >= 0 && dev < 64, CQ_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    CQ_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = static_cast<uint64_t*>(p);
+  }
+  return g_noalloc_addr[dev];
+}
+}  // namespace
+
+int guarded_call(const std::function<void()>& f);   // capi.cpp: exceptions to status codes
+
 }  // namespace cqb
+
+extern "C" int cq_exact_dots_noalloc(int count, const double* const* x_dev, const double* const* y_dev,
+                                     const int64_t* n, void* stream, double* out) {
+  using namespace cqb;
+  return guarded_call([&] {
+    CQ_CHECK(x_dev && n && out, CQ_ERR_ARG, "null argument");
+    CQ_CHECK(count >= 1 && count <= kNoAllocSums, CQ_ERR_ARG,
+             "cq_exact_dots_noalloc: count must be 1..CQ_NOALLOC_MAX_SUMS (8) sums per call");
+    for (int k = 0; k < count; ++k) CQ_CHECK(n[k] >= 0 && (x_dev[k] || n[k] == 0), CQ_ERR_ARG, "bad operand");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    uint64_t* base = noalloc_scratch();
+    uint64_t* part = base;
+    uint64_t* res = base + 3 * kRedBlocks;
+    int* flags = reinterpret_cast<int*>(base + 3 * kRedBlocks + 4 * kNoAllocSums);
+    // the pass-1 flags (largest exponent, non-finite) start at zero; the partials and results
+    // are overwritten by every call
+    CQ_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * 2 * count, st));
+    for (int k = 0; k < count; ++k) {
+      const double* x = x_dev[k];
+      const double* y = y_dev ? y_dev[k] : nullptr;
+      const int g = acc_grid(n[k]);
+      k_acc_emax<<<g, kT, 0, st>>>(x, y, n[k], flags + 2 * k, flags + 2 * k + 1);
+      k_acc_sum<<<g, kT, 0, st>>>(x, y, n[k], flags + 2 * k, part);
+      k_acc_final<<<1, kT, 0, st>>>(part, g, flags + 2 * k, res + 4 * k);
+    }
+    CQ_CUDA(cudaGetLastError());
+    uint64_t w[4 * kNoAllocSums];
+    CQ_CUDA(cudaMemcpyAsync(w, res, sizeof(uint64_t) * 4 * count, cudaMemcpyDeviceToHost, st));
+    CQ_CUDA(cudaStreamSynchronize(st));
+    for (int k = 0; k < count; ++k) out[k] = exact_sum_value(&w[4 * k]);
+  });
+}
+

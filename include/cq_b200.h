@@ -257,6 +257,26 @@ int cq_lnv_solve(cq_lnv* s, cq_lnv_result* res);
  */
 int cq_lnv_solve_host(cq_lnv* s, const double* S, const double* H, double* L_out, double* K_out, cq_lnv_result* res);
 
+/*
+ * Exact dot products that allocate nothing (no counterpart in the reference).  For callers that
+ * cannot allocate device memory when they need a trace: a Fortran/MPI host that has handed the
+ * whole device to its own memory pool, or a latency-critical loop that must not take the
+ * device-wide synchronisation cudaMalloc/cudaFree can imply.  out[k] = sum_i x_dev[k][i] *
+ * y_dev[k][i] over n[k] elements (a plain sum where y_dev is NULL or y_dev[k] is NULL), with the
+ * same exact, order-independent rounding as cq_matrix_product_trace, so the values are
+ * bit-identical to it.  x_dev / y_dev are host arrays of device pointers; work is enqueued on
+ * `stream` (a cudaStream_t, NULL = the default stream) and the call synchronises it.
+ *   - At most CQ_NOALLOC_MAX_SUMS sums per call; more is rejected with CQ_ERR_ARG.
+ *   - The scratch is one static device array of 28.7 KiB that every GPU loading the library
+ *     holds until exit.  The first call on each device looks up that array's device address;
+ *     make it before any stream capture on that device.
+ *   - Every call shares the array: calls that overlap on the GPU (two streams, two threads) race
+ *     and give wrong sums.  Serialise them.
+ */
+#define CQ_NOALLOC_MAX_SUMS 8
+int cq_exact_dots_noalloc(int count, const double* const* x_dev, const double* const* y_dev, const int64_t* n,
+                          void* stream, double* out);
+
 /* Reduction log (tracing): with enable = 1 every later trace and product trace of the chain
  * (matrix_trace / matrix_product_trace values, in call order) is recorded.  Each call returns
  * the values recorded so far (*n of them, at most cap copied to out), clears the log and sets
