@@ -225,7 +225,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="lnv512", choices=["lnv512", "batch", "serve", "mult216", "mult512"],
+    ap.add_argument("--workload", default="lnv512", choices=["lnv512", "batch", "serve", "mult216", "mult512", "mult4096"],
                     help="lnv512: the plain FP64 512-atom solve (default); batch / serve: mixed-precision solves of "
                          "many systems on concurrent slots vs the FP64 path one at a time; mult216 / mult512: single "
                          "block products (216-atom DZP C=A.B; the products of one 512-atom LNV call)")
@@ -238,7 +238,7 @@ def main():
     ap.add_argument("--rate", type=float, default=200.0)
     args = ap.parse_args()
     ws, rank, local = dist_env()
-    if args.workload in ("mult216", "mult512") and args.impl == "ours":
+    if args.workload in ("mult216", "mult512", "mult4096") and args.impl == "ours":
         if rank == 0:
             mult_main(args)
         return
@@ -495,15 +495,23 @@ def mult_main(args):
         prods = [("A.B->C", 1, 0, 1, 2, a, b, c)]
         desc = "216-atom Si DZP (13x13), A 8 / B 12 / C 20 bohr"
     else:
-        prob = build_problem(cq_b200)
-        g, ridx = prob["system"], prob["ridx"]
-        rs = np.random.default_rng(3)
-        mats = {k: torch.from_numpy(rs.uniform(-0.1, 0.1, g.length(ridx[k]))).to(dev) for k in
-                ("S", "H", "L", "LS", "LH", "LSL", "SLS")}
+        from cq_b200 import inputs as _inp
+        ncell, nsf = (4, 4) if args.workload == "mult512" else (8, 13)
+        coords, cell = _inp.diamond_si(ncell, sigma=0.1, seed=2)
+        n = len(coords)
+        rng = cq_b200.lnv_ranges(CFG["rs"], CFG["rh"], CFG["rl"], CFG["rt"])
+        ridx = {k: i for i, k in enumerate(rng)}
+        g = cq_b200.System(coords, cell, np.full(n, nsf, np.int32), list(rng.values()))
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(3)
+        mats = {k: (torch.rand(g.length(ridx[k]), dtype=torch.float64, device=dev, generator=gen) - 0.5) * 0.2
+                for k in ("S", "H", "L", "LS", "LH", "LSL", "SLS")}
         prods = []
         for (t, x, y, z) in lnv_call_products():
             prods.append(("%s_%s_%s/%d" % (x, y, z, t), t, ridx[x], ridx[y], ridx[z], mats[x], mats[y], mats[z]))
-        desc = "512-atom Si SZ (4x4), the nine products of one LNV call"
+        desc = "%d-atom Si %s, S/H/L/T ranges 10/12/16/10 bohr: the nine products of one LNV call" % (
+            n, "SZ (4x4)" if nsf == 4 else "DZP (13x13)")
+    torch.cuda.synchronize()
     g.set_stream(stream.cuda_stream)
     if args.variant is not None:
         g.set_mult_variant(args.variant)

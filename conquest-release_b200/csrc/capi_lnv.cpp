@@ -64,6 +64,7 @@ int cq_lnv_params_default(cq_lnv_params* p) {
   p->max_outer = 40;
   p->mixed = 0;
   p->mixed_tolerance = 1.0e-5;
+  p->fp64_mcw_sweeps = 0;
   return CQ_OK;
 }
 

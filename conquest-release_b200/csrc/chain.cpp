@@ -93,18 +93,22 @@ void LNVSolver::mult_dispatch(ProductPlan& P, double* a, const double* b, double
 void LNVSolver::solve() {
   stats = LNVStats();
   delta_e = 0.0;
+  // every solve starts from the state of a new solver: the matrices the chain carries from one
+  // call to the next (L, phi, K, T and the products of L) are cleared
+  for (DMat* m : {&L, &T, &Ttran, &LS, &SL, &K, &phi})
+    CQ_CUDA(cudaMemsetAsync(m->p, 0, sizeof(double) * std::max<int64_t>(m->n, 1), S.stream));
+  use_mixed = false;
+  invert_S();                       // T = S^-1 in FP64 in both forms
   if (!prm.mixed) {
-    use_mixed = false;
-    invert_S();
     find_min_dm(true);
     return;
   }
-  // split-precision phase to the hand-over residual, then FP64 from that L to the final tolerance
+  // split-precision phase to the hand-over residual, optional FP64 McWeeny purification sweeps,
+  // then FP64 FindMinDM from that L to the final tolerance
   const double tol = prm.tolerance;
   use_mixed = true;
   prm.tolerance = prm.mixed_tolerance;
   try {
-    invert_S();
     find_min_dm(true);
   } catch (...) {
     prm.tolerance = tol;
@@ -114,7 +118,22 @@ void LNVSolver::solve() {
   prm.tolerance = tol;
   use_mixed = false;
   stats.converged = 0;
+  if (prm.fp64_mcw_sweeps > 0) purify(prm.fp64_mcw_sweeps);
   find_min_dm(false);
+}
+
+// McWeeny purification sweeps of L (McW_matrix_multiply_nonds, McWeeny.f90:620-740), kept while
+// the purification parameter c stays in [0, 1].
+void LNVSolver::purify(int sweeps) {
+  DMat RhoNew = temp(RL);
+  for (int n = 0; n < sweeps; ++n) {
+    double omega, cn;
+    mcw_mm_nonds(RhoNew, omega, cn);
+    if (cn > 1.0 || cn < 0.0) break;
+    msum(0.0, L, 1.0, RhoNew);
+    symmetrise_L();
+    stats.mcw_sweeps++;
+  }
 }
 
 void LNVSolver::msum(double alpha, DMat& A, double beta, const DMat& B) {

@@ -72,6 +72,7 @@ class LNVSolver {
   // complete solve: T = S^-1, FindMinDM from the McWeeny start; with prm.mixed the products run in
   // split precision until the residual reaches prm.mixed_tolerance, then FindMinDM continues in FP64
   void solve();
+  void purify(int sweeps);
   bool use_mixed = false;   // current product arithmetic of mult_dispatch
   static void do_pulay(int iPulay, const double* Aij, int n, int max_n, double* al);
   void lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim, double* electrons, double* energy);

@@ -203,6 +203,7 @@ struct ProductPlan {
   DevBuf<int2> pairs;             // [n_pairs] (x block, b block)
   int n_tiles = 0;                // row tiles of the staged 4x4 kernel: (q0, q1, x row first, x row end)
   DevBuf<int4> tiles;
+  DevBuf<int> order;              // output blocks by descending pair count (warp-staged 4x4 kernel)
 };
 
 // Split-precision tensor-core product: pair lists sorted by the first operand block,
@@ -260,7 +261,8 @@ struct System {
   DevBuf<double> diag_buf;        // gathered onsite diagonal (exact trace)
   int64_t launches = 0;           // kernels launched by this system (all kinds)
   int mult_variant = 1;           // 4x4 FP64 product kernel: 0 = one lane per element, 1 = one thread per block,
-                                  // 2 = one thread per block with the operand row staged in shared memory
+                                  // 2 = one thread per block with the operand row staged in shared memory,
+                                  // 3 = one thread per block with warp-cooperative staging of the operand blocks
   bool blocking_sync = false;     // host waits sleep on a blocking-sync event instead of spinning
   cudaEvent_t sync_ev = nullptr;
   ProductProfile prof;

@@ -14,6 +14,9 @@
 //
 // The bound is the L2/HBM traffic of the operand blocks (an nd x nd FP64 block
 // pair per triple, 2 nd^3 flops): for nd = 4 this is 256 B per 128 flops.
+#include <algorithm>
+#include <numeric>
+
 #include "cq_internal.hpp"
 
 namespace cqb {
@@ -249,6 +252,90 @@ __global__ void __launch_bounds__(128) k_mult_nd4_rows(MultArgs M, const int4* _
   }
 }
 
+// 4 x 4 blocks, one thread per output block, operand blocks staged through shared memory by
+// the whole warp.  A thread-per-block kernel that reads its own operand blocks issues 16-byte
+// loads that touch 32 different blocks per warp instruction, which saturates the L1 on
+// wavefronts long before the FP64 pipe is busy.  Here, per step, the warp first copies the 32
+// (x, b) block pairs its lanes need with loads in which 8 consecutive lanes read one whole
+// 128-byte block (4 blocks per instruction), stores them in padded shared memory (9 x 16 bytes
+// per block: conflict-free 16-byte reads per quarter warp), then every lane does its own 4 x 4
+// product in the reference order.  Output blocks are taken in `order` (descending pair count)
+// so the lanes of a warp have pair lists of similar length.
+template <int TYPE, bool EXACT>
+__global__ void __launch_bounds__(128, 5) k_mult_nd4_warp(MultArgs M, const int* __restrict__ order) {
+  constexpr int kStride = 9;   // double2 per staged block (8 + 1 padding)
+  __shared__ double2 sx[4][32 * kStride];
+  __shared__ double2 sb[4][32 * kStride];
+  const unsigned kFull = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int base = (blockIdx.x * 4 + warp) * 32;
+  if (base >= M.n_out) return;                  // whole warp
+  const int slot = base + lane;
+  const bool has = slot < M.n_out;
+  const int q = has ? order[slot] : 0;
+  int64_t t = has ? M.ptr[q] : 0, tend = has ? M.ptr[q + 1] : 0;
+  double acc[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+  double2* X = sx[warp];
+  double2* B = sb[warp];
+  const double2* Xg = reinterpret_cast<const double2*>(M.x);
+  const double2* Bg = reinterpret_cast<const double2*>(M.b);
+  const int chunk = lane & 7;
+  while (__any_sync(kFull, t < tend)) {
+    const bool act = t < tend;
+    const int2 pr = act ? M.pairs[t] : make_int2(-1, -1);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int src = 4 * j + (lane >> 3);
+      const int xb = __shfl_sync(kFull, pr.x, src);
+      const int bb = __shfl_sync(kFull, pr.y, src);
+      if (xb >= 0) {
+        X[src * kStride + chunk] = __ldg(Xg + (int64_t)xb * 8 + chunk);
+        B[src * kStride + chunk] = __ldg(Bg + (int64_t)bb * 8 + chunk);
+      }
+    }
+    __syncwarp();
+    if (act) {
+      double x[16], b[16];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {
+        const double2 xv = X[lane * kStride + v], bv = B[lane * kStride + v];
+        x[2 * v] = xv.x; x[2 * v + 1] = xv.y;
+        b[2 * v] = bv.x; b[2 * v + 1] = bv.y;
+      }
+      if (TYPE == 1) {
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+          for (int n1 = 0; n1 < 4; ++n1) {
+            double a = acc[n1 + 4 * m];
+#pragma unroll
+            for (int n3 = 0; n3 < 4; ++n3) a = madd<EXACT>(a, x[n1 + 4 * n3], b[n3 + 4 * m]);
+            acc[n1 + 4 * m] = a;
+          }
+      } else {
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+          for (int n1 = 0; n1 < 4; ++n1) {
+            double a = acc[n1 + 4 * m];
+#pragma unroll
+            for (int n2 = 0; n2 < 4; ++n2) a = madd<EXACT>(a, x[n1 + 4 * n2], b[m + 4 * n2]);
+            acc[n1 + 4 * m] = a;
+          }
+      }
+      ++t;
+    }
+    __syncwarp();
+  }
+  if (has) {
+    double2* O2 = reinterpret_cast<double2*>(M.out + 16 * (int64_t)q);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) O2[v] = make_double2(acc[2 * v], acc[2 * v + 1]);
+  }
+}
+
 // One drop-in m_kern_max (type 1) / m_kern_min (type 2) call: output blocks with explicit
 // offsets, accumulated in place in the layouts mat_mult passes (type 1 reads the local
 // transpose a(n3 + nd3*n1); type 2 accumulates into it).  One warp per output block.
@@ -318,7 +405,24 @@ void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, doub
   S.launches++;
   // the 4 x 4 path reads B with 16-byte vector loads: require 16-byte aligned operands
   bool aligned = ((uintptr_t)b % 16 == 0) && ((uintptr_t)M.x % 16 == 0) && ((uintptr_t)M.out % 16 == 0);
-  if (S.uniform_nsf == 4 && aligned && S.mult_variant == 2) {
+  if (S.uniform_nsf == 4 && aligned && S.mult_variant == 3) {
+    if (P.order.n == 0) {
+      // output blocks by descending pair count (stable): lanes of a warp get similar list lengths
+      std::vector<int64_t> ptr = P.ptr.download(st);
+      std::vector<int> ord(M.n_out);
+      std::iota(ord.begin(), ord.end(), 0);
+      std::stable_sort(ord.begin(), ord.end(), [&](int u, int v) { return ptr[u + 1] - ptr[u] > ptr[v + 1] - ptr[v]; });
+      P.order.upload(ord, st);
+    }
+    const int grid = (M.n_out + 127) / 128;
+    if (P.mult_type == 1) {
+      if (exact) k_mult_nd4_warp<1, true><<<grid, 128, 0, st>>>(M, P.order.p);
+      else k_mult_nd4_warp<1, false><<<grid, 128, 0, st>>>(M, P.order.p);
+    } else {
+      if (exact) k_mult_nd4_warp<2, true><<<grid, 128, 0, st>>>(M, P.order.p);
+      else k_mult_nd4_warp<2, false><<<grid, 128, 0, st>>>(M, P.order.p);
+    }
+  } else if (S.uniform_nsf == 4 && aligned && S.mult_variant == 2) {
     constexpr int kChunk = 256;                 // 32 KiB of operand blocks per chunk
     if (P.n_tiles == 0) {
       // tiles: up to 128 output blocks of one row, with that row's range of operand blocks

@@ -202,9 +202,11 @@ typedef struct {
   int max_outer;           /* bound on FindMinDM outer passes (40); the reference loops until done, which a
                               residual stalled above `tolerance` never reaches: the solve then stops with
                               converged = 0 */
-  int mixed;               /* 1: cq_lnv_solve runs Hotelling and FindMinDM with CQ_PREC_BF16X3 products, then
-                              continues FindMinDM from that L with FP64 products to `tolerance` */
+  int mixed;               /* 1: cq_lnv_solve runs FindMinDM (McWeeny start included) with CQ_PREC_BF16X3
+                              products to `mixed_tolerance`, then continues from that L with FP64 products
+                              to `tolerance`; Hotelling, traces, line search and Pulay stay FP64 */
   double mixed_tolerance;  /* residual at which the split-precision phase hands over to FP64 */
+  int fp64_mcw_sweeps;     /* FP64 McWeeny purification sweeps of L between the two phases (0) */
 } cq_lnv_params;
 
 typedef struct {
