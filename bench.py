@@ -110,6 +110,27 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def fp64_peak_tflops(dev):
+    """FP64 reference peak on this GPU, measured here: cuBLAS DGEMM (torch.matmul float64) 8192^3,
+    best of 5 after 2 warm-ups (CUDA events)."""
+    import torch
+    n = 8192
+    a = torch.rand(n, n, dtype=torch.float64, device=dev)
+    b = torch.rand(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
+
+
 def load_traffic():
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary (None if absent)."""
     p = os.path.join(ROOT, "profiles", "lnv512_mult_traffic.json")
@@ -230,7 +251,9 @@ def main():
                          "many systems on concurrent slots vs the FP64 path one at a time; mult216 / mult512: single "
                          "block products (216-atom DZP C=A.B; the products of one 512-atom LNV call)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3"])
-    ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (0, 1, 2)")
+    ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (-1 autotuned, 0..3)")
+    ap.add_argument("--one-solve", action="store_true",
+                    help="run exactly one solve of the workload and print its result (for launch lists under ncu)")
     ap.add_argument("--requests", type=int, default=32)
     ap.add_argument("--nmin", type=int, default=64)
     ap.add_argument("--nmax", type=int, default=1000)
@@ -268,12 +291,17 @@ def main():
     dev = torch.device("cuda", local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # 256 MB > 126 MB L2
     solver.set_SH(prob["S"], prob["H"])
+    if args.one_solve:
+        r = solver.solve()
+        torch.cuda.synchronize()
+        emit({"one_solve": {k: r[k] for k in ("energy", "electrons", "converged", "n_products")},
+              "gpu_launches": system.launch_count()})
+        return
     for _ in range(args.warmup):
         res = solver.solve()
     torch.cuda.synchronize()
-    # ---- timed region: K solves on device-resident S, H
+    # ---- timed region: K solves on device-resident S, H (no per-kernel events inside)
     launches0 = system.launch_count()
-    system.profile(True)
     step_ms = []
     if dist:
         dist.barrier()
@@ -294,9 +322,19 @@ def main():
         dist.barrier()
     total_ms = ev_all0.elapsed_time(ev_all1)
     steps_ms = [a.elapsed_time(b) for a, b in step_ms]
+    launches = system.launch_count() - launches0
+    # ---- one more solve with CUDA events around every product launch (kernel-level numbers)
+    system.profile(True)
+    flush.zero_()
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    solver.solve()
+    p1.record(stream)
+    torch.cuda.synchronize()
+    prof_step_ms = p0.elapsed_time(p1)
     prof = system.profile_read()
     system.profile(False)
-    launches = system.launch_count() - launches0
     t_max = total_ms
     if dist:
         t = torch.tensor([total_ms], device=dev)
@@ -327,6 +365,7 @@ def main():
         peak, peak_kind = load_peaks()
         achieved = prof["bytes"] / (prof["ms"] / 1e3) / 1e9 if prof["ms"] > 0 else 0.0
         traffic = load_traffic()
+        dgemm = fp64_peak_tflops(dev)
         per_solve_flops = res["flops"]
         fl_call = flops_of_lnv_call(system, prob["ridx"])
         rec = {"workload": WORKLOAD, "flops_per_solve": per_solve_flops, "products_per_solve": res["n_products"],
@@ -356,16 +395,21 @@ def main():
                       "flops": per_solve_flops, "late_iters": res["late_iters"], "early_iters": res["early_iters"],
                       "mcw_sweeps": res["mcw_sweeps"], "converged": res["converged"]},
             "block_mult_tflops": (prof["flops"] / (prof["ms"] / 1e3) / 1e12) if prof["ms"] > 0 else None,
-            "roofline": {"bound": "hbm", "kernel": "k_mult_nd4 (FP64 4x4 block products)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "FP64 4x4 block products (autotuned k_mult_nd4_warp / k_mult_nd4_tpb)", "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "launches": prof["launches"],
                          "avg_launch_ms": prof["ms"] / max(1, prof["launches"]),
                          "algorithmic_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]),
-                         "share_of_step": prof["ms"] / total_ms if total_ms > 0 else None},
+                         "share_of_step": prof["ms"] / prof_step_ms if prof_step_ms > 0 else None,
+                         "measured_in": "one extra solve with CUDA events around every product launch"},
+            "roofline_fp64": {"bound": "fp64", "achieved": (prof["flops"] / (prof["ms"] / 1e3) / 1e12) if prof["ms"] > 0 else None,
+                              "peak": dgemm, "peak_kind": "measured here: cuBLAS DGEMM 8192^3", "unit": "TFLOP/s",
+                              "frac": ((prof["flops"] / (prof["ms"] / 1e3) / 1e12) / dgemm) if prof["ms"] > 0 else None},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 8 * (prob["S"].size + prob["H"].size),
                     "d2h_bytes_per_step": 8 * (nL + nK)},
             "gpu_launches": launches,
+            "gpu_launches_per_step": launches / max(1, args.steps),
             "clocks": clocks,
         }
         emit(line)

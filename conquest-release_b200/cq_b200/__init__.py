@@ -248,7 +248,8 @@ class System:
         check(lib().cq_system_set_stream(self._h, c_void_p(stream) if stream else None))
 
     def set_mult_variant(self, v):
-        """FP64 4x4 product kernel: 0 = one lane per output element, 1 = one thread per output block."""
+        """FP64 4x4 product kernel: -1 = autotuned per product (default), 0 = one lane per output element,
+        1 = one thread per output block, 2 = operand row staged in shared memory, 3 = warp-staged operand blocks."""
         check(lib().cq_system_set_option(self._h, 1, int(v)))
 
     def profile(self, on=True):

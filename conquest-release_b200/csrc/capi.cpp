@@ -286,7 +286,7 @@ int cq_system_set_option(cq_system* sys, int option, int value) {
   return guarded([&] {
     check_sys(sys);
     if (option == CQ_OPT_MULT_VARIANT) {
-      CQ_CHECK(value >= 0 && value <= 3, CQ_ERR_ARG, "mult variant must be 0..3");
+      CQ_CHECK(value >= -1 && value <= 3, CQ_ERR_ARG, "mult variant must be -1 (autotuned) or 0..3");
       sys->S.mult_variant = value;
     } else if (option == CQ_OPT_BLOCKING_SYNC) {
       sys->S.blocking_sync = value != 0;

@@ -193,6 +193,8 @@ struct RangeIndex {
 
 // Per-product pair lists: for each output block, the ordered list of
 // (first operand block, B block) pairs in the reference's summation order.
+constexpr int kVariantAuto = -1;
+
 struct ProductPlan {
   int mult_type = 1;
   int ra = -1, rb = -1, rc = -1;  // mat_mult roles: a (A or type-2 output), b, c (C or type-2 input)
@@ -204,6 +206,8 @@ struct ProductPlan {
   int n_tiles = 0;                // row tiles of the staged 4x4 kernel: (q0, q1, x row first, x row end)
   DevBuf<int4> tiles;
   DevBuf<int> order;              // output blocks by descending pair count (warp-staged 4x4 kernel)
+  int tuned = -1;                 // FP64 kernel variant chosen by the autotuner (-1: not tuned yet)
+  float tune_ms[4] = {0, 0, 0, 0};
 };
 
 // Split-precision tensor-core product: pair lists sorted by the first operand block,
@@ -260,7 +264,8 @@ struct System {
   DevBuf<int> diag_off;           // first onsite-diagonal slot of each primary atom
   DevBuf<double> diag_buf;        // gathered onsite diagonal (exact trace)
   int64_t launches = 0;           // kernels launched by this system (all kinds)
-  int mult_variant = 1;           // 4x4 FP64 product kernel: 0 = one lane per element, 1 = one thread per block,
+  int mult_variant = -1;          // 4x4 FP64 product kernel: -1 = chosen per product by the autotuner,
+                                  // 0 = one lane per element, 1 = one thread per block,
                                   // 2 = one thread per block with the operand row staged in shared memory,
                                   // 3 = one thread per block with warp-cooperative staging of the operand blocks
   bool blocking_sync = false;     // host waits sleep on a blocking-sync event instead of spinning

@@ -380,6 +380,105 @@ void launch_dropin(int type, const int64_t* d_out, const int* d_dims, const int6
   CQ_CUDA(cudaGetLastError());
 }
 
+// One launch of the FP64 product with kernel `variant` (0..3 for uniform 4 x 4 blocks with
+// 16-byte aligned operands; anything else runs the generic kernel).  All variants give the same
+// bits: they differ only in how the work is mapped onto the GPU.
+static void launch_variant(System& S, ProductPlan& P, const MultArgs& M, int variant, int exact, bool nd4) {
+  cudaStream_t st = S.stream;
+  const int T = 256;
+  RangeIndex& O = P.mult_type == 1 ? *S.ranges[P.rc] : *S.ranges[P.ra];
+  RangeIndex& X = P.mult_type == 1 ? *S.ranges[P.ra] : *S.ranges[P.rc];
+  if (nd4 && variant == 3) {
+    if (P.order.n == 0) {
+      // output blocks by descending pair count (stable): lanes of a warp get similar list lengths
+      std::vector<int64_t> ptr = P.ptr.download(st);
+      std::vector<int> ord(M.n_out);
+      std::iota(ord.begin(), ord.end(), 0);
+      std::stable_sort(ord.begin(), ord.end(), [&](int u, int v) { return ptr[u + 1] - ptr[u] > ptr[v + 1] - ptr[v]; });
+      P.order.upload(ord, st);
+    }
+    const int grid = (M.n_out + 127) / 128;
+    if (P.mult_type == 1) {
+      if (exact) k_mult_nd4_warp<1, true><<<grid, 128, 0, st>>>(M, P.order.p);
+      else k_mult_nd4_warp<1, false><<<grid, 128, 0, st>>>(M, P.order.p);
+    } else {
+      if (exact) k_mult_nd4_warp<2, true><<<grid, 128, 0, st>>>(M, P.order.p);
+      else k_mult_nd4_warp<2, false><<<grid, 128, 0, st>>>(M, P.order.p);
+    }
+  } else if (nd4 && variant == 2) {
+    constexpr int kChunk = 256;                 // 32 KiB of operand blocks per chunk
+    if (P.n_tiles == 0) {
+      // tiles: up to 128 output blocks of one row, with that row's range of operand blocks
+      std::vector<int4> tl;
+      for (int i = 0; i < S.geo.n_prim; ++i)
+        for (int q0 = O.h_row_ptr[i]; q0 < O.h_row_ptr[i + 1]; q0 += 128)
+          tl.push_back(make_int4(q0, std::min(q0 + 128, O.h_row_ptr[i + 1]), X.h_row_ptr[i], X.h_row_ptr[i + 1]));
+      P.tiles.upload(tl, st);
+      P.n_tiles = (int)tl.size();
+    }
+    if (P.mult_type == 1) {
+      if (exact) k_mult_nd4_rows<1, true, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
+      else k_mult_nd4_rows<1, false, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
+    } else {
+      if (exact) k_mult_nd4_rows<2, true, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
+      else k_mult_nd4_rows<2, false, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
+    }
+  } else if (nd4 && variant == 1) {
+    const int T1 = 128;
+    int grid = (M.n_out + T1 - 1) / T1;
+    if (P.mult_type == 1) {
+      if (exact) k_mult_nd4_tpb<1, true><<<grid, T1, 0, st>>>(M); else k_mult_nd4_tpb<1, false><<<grid, T1, 0, st>>>(M);
+    } else {
+      if (exact) k_mult_nd4_tpb<2, true><<<grid, T1, 0, st>>>(M); else k_mult_nd4_tpb<2, false><<<grid, T1, 0, st>>>(M);
+    }
+  } else if (nd4) {
+    int grid = (int)(((int64_t)M.n_out * 16 + T - 1) / T);
+    if (P.mult_type == 1) {
+      if (exact) k_mult_nd4<1, true><<<grid, T, 0, st>>>(M); else k_mult_nd4<1, false><<<grid, T, 0, st>>>(M);
+    } else {
+      if (exact) k_mult_nd4<2, true><<<grid, T, 0, st>>>(M); else k_mult_nd4<2, false><<<grid, T, 0, st>>>(M);
+    }
+  } else {
+    int grid = (int)(((int64_t)M.n_out * 32 + T - 1) / T);
+    if (P.mult_type == 1) {
+      if (exact) k_mult_generic<1, true><<<grid, T, 0, st>>>(M); else k_mult_generic<1, false><<<grid, T, 0, st>>>(M);
+    } else {
+      if (exact) k_mult_generic<2, true><<<grid, T, 0, st>>>(M); else k_mult_generic<2, false><<<grid, T, 0, st>>>(M);
+    }
+  }
+  S.launches++;
+  CQ_CUDA(cudaGetLastError());
+}
+
+// Autotuner: on the first call of a product, time each candidate kernel (one warm launch, then
+// one launch between CUDA events on the system's stream) and keep the fastest for the plan.  The
+// candidates give identical bits and each fully overwrites the output, so tuning changes speed
+// only; the last timed launch leaves the correct result.
+static int tuned_variant(System& S, ProductPlan& P, const MultArgs& M, int exact) {
+  if (P.tuned >= 0) return P.tuned;
+  static const int kCands[] = {1, 3};
+  cudaEvent_t e0, e1;
+  CQ_CUDA(cudaEventCreate(&e0));
+  CQ_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int pick = 3;
+  for (int v : kCands) {
+    launch_variant(S, P, M, v, exact, true);
+    CQ_CUDA(cudaEventRecord(e0, S.stream));
+    launch_variant(S, P, M, v, exact, true);
+    CQ_CUDA(cudaEventRecord(e1, S.stream));
+    CQ_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    P.tune_ms[v] = ms;
+    if (ms < best) { best = ms; pick = v; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  P.tuned = pick;
+  return pick;
+}
+
 void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, double* c, int exact) {
   RangeIndex &A = *S.ranges[P.ra], &B = *S.ranges[P.rb], &C = *S.ranges[P.rc];
   MultArgs M;
@@ -399,71 +498,14 @@ void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, doub
   M.out = P.mult_type == 1 ? c : a;
   if (M.n_out == 0) return;
   cudaStream_t st = S.stream;
-  const int T = 256;
+  // the 4 x 4 kernels read blocks with 16-byte vector loads: require 16-byte aligned operands
+  const bool aligned = ((uintptr_t)b % 16 == 0) && ((uintptr_t)M.x % 16 == 0) && ((uintptr_t)M.out % 16 == 0);
+  const bool nd4 = S.uniform_nsf == 4 && aligned;
+  int variant = S.mult_variant;
+  if (nd4 && variant == kVariantAuto) variant = tuned_variant(S, P, M, exact);
   cudaEvent_t ev0 = nullptr;
   if (S.prof.on) { ev0 = S.prof.get(); CQ_CUDA(cudaEventRecord(ev0, st)); }
-  S.launches++;
-  // the 4 x 4 path reads B with 16-byte vector loads: require 16-byte aligned operands
-  bool aligned = ((uintptr_t)b % 16 == 0) && ((uintptr_t)M.x % 16 == 0) && ((uintptr_t)M.out % 16 == 0);
-  if (S.uniform_nsf == 4 && aligned && S.mult_variant == 3) {
-    if (P.order.n == 0) {
-      // output blocks by descending pair count (stable): lanes of a warp get similar list lengths
-      std::vector<int64_t> ptr = P.ptr.download(st);
-      std::vector<int> ord(M.n_out);
-      std::iota(ord.begin(), ord.end(), 0);
-      std::stable_sort(ord.begin(), ord.end(), [&](int u, int v) { return ptr[u + 1] - ptr[u] > ptr[v + 1] - ptr[v]; });
-      P.order.upload(ord, st);
-    }
-    const int grid = (M.n_out + 127) / 128;
-    if (P.mult_type == 1) {
-      if (exact) k_mult_nd4_warp<1, true><<<grid, 128, 0, st>>>(M, P.order.p);
-      else k_mult_nd4_warp<1, false><<<grid, 128, 0, st>>>(M, P.order.p);
-    } else {
-      if (exact) k_mult_nd4_warp<2, true><<<grid, 128, 0, st>>>(M, P.order.p);
-      else k_mult_nd4_warp<2, false><<<grid, 128, 0, st>>>(M, P.order.p);
-    }
-  } else if (S.uniform_nsf == 4 && aligned && S.mult_variant == 2) {
-    constexpr int kChunk = 256;                 // 32 KiB of operand blocks per chunk
-    if (P.n_tiles == 0) {
-      // tiles: up to 128 output blocks of one row, with that row's range of operand blocks
-      std::vector<int4> tl;
-      for (int i = 0; i < S.geo.n_prim; ++i)
-        for (int q0 = O.h_row_ptr[i]; q0 < O.h_row_ptr[i + 1]; q0 += 128)
-          tl.push_back(make_int4(q0, std::min(q0 + 128, O.h_row_ptr[i + 1]), X.h_row_ptr[i], X.h_row_ptr[i + 1]));
-      P.tiles.upload(tl, st);
-      P.n_tiles = (int)tl.size();
-    }
-    if (P.mult_type == 1) {
-      if (exact) k_mult_nd4_rows<1, true, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
-      else k_mult_nd4_rows<1, false, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
-    } else {
-      if (exact) k_mult_nd4_rows<2, true, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
-      else k_mult_nd4_rows<2, false, kChunk><<<P.n_tiles, 128, 0, st>>>(M, P.tiles.p);
-    }
-  } else if (S.uniform_nsf == 4 && aligned && S.mult_variant == 1) {
-    const int T1 = 128;
-    int grid = (M.n_out + T1 - 1) / T1;
-    if (P.mult_type == 1) {
-      if (exact) k_mult_nd4_tpb<1, true><<<grid, T1, 0, st>>>(M); else k_mult_nd4_tpb<1, false><<<grid, T1, 0, st>>>(M);
-    } else {
-      if (exact) k_mult_nd4_tpb<2, true><<<grid, T1, 0, st>>>(M); else k_mult_nd4_tpb<2, false><<<grid, T1, 0, st>>>(M);
-    }
-  } else if (S.uniform_nsf == 4 && aligned) {
-    int grid = (int)(((int64_t)M.n_out * 16 + T - 1) / T);
-    if (P.mult_type == 1) {
-      if (exact) k_mult_nd4<1, true><<<grid, T, 0, st>>>(M); else k_mult_nd4<1, false><<<grid, T, 0, st>>>(M);
-    } else {
-      if (exact) k_mult_nd4<2, true><<<grid, T, 0, st>>>(M); else k_mult_nd4<2, false><<<grid, T, 0, st>>>(M);
-    }
-  } else {
-    int grid = (int)(((int64_t)M.n_out * 32 + T - 1) / T);
-    if (P.mult_type == 1) {
-      if (exact) k_mult_generic<1, true><<<grid, T, 0, st>>>(M); else k_mult_generic<1, false><<<grid, T, 0, st>>>(M);
-    } else {
-      if (exact) k_mult_generic<2, true><<<grid, T, 0, st>>>(M); else k_mult_generic<2, false><<<grid, T, 0, st>>>(M);
-    }
-  }
-  CQ_CUDA(cudaGetLastError());
+  launch_variant(S, P, M, variant, exact, nd4);
   if (S.prof.on) {
     cudaEvent_t ev1 = S.prof.get();
     CQ_CUDA(cudaEventRecord(ev1, st));

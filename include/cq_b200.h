@@ -169,9 +169,12 @@ int cq_launch_count(cq_system* sys, int64_t* count);
  * hamiltonian_H up to the last bit of exp(). */
 int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out);
 
-/* Tuning options.  CQ_OPT_MULT_VARIANT: FP64 4x4 product kernel, 0 = one lane per output
- * element, 1 = one thread per output block (default), 2 = one thread per output block with the
- * first operand's row staged in shared memory.  All give identical results.
+/* Tuning options.  CQ_OPT_MULT_VARIANT: FP64 4x4 product kernel, -1 = chosen per product by the
+ * autotuner (default: the first call of each product times the candidates 1 and 3 with CUDA
+ * events and keeps the faster), 0 = one lane per output element, 1 = one thread per output
+ * block, 2 = one thread per output block with the first operand's row staged in shared memory,
+ * 3 = one thread per output block with the warp staging the operand blocks through shared
+ * memory.  All give identical results.
  * CQ_OPT_BLOCKING_SYNC: 1 = the host thread sleeps on a blocking-sync event whenever the
  * solver waits for a scalar from the device (many concurrent solvers per host core), 0 = it
  * spins in cudaStreamSynchronize (default, lowest latency for one solver). */
