@@ -577,7 +577,9 @@ def mult_main(args):
                 ms.append(e0.elapsed_time(e1))
             m = float(np.median(ms))
             nbytes = 8.0 * (g.length(ra) + g.length(rb) + g.length(rc))
-            out.append({"product": name, "triples": triples, "flops": flops, "ms": m,
+            tv, tms = g.product_tuning(t, ra, rb, rc)
+            out.append({"product": name, "triples": triples, "flops": flops, "ms": m, "tuned_variant": tv,
+                        "tune_ms": tms,
                         "tflops": flops / (m / 1e3) / 1e12, "gbs_algorithmic": nbytes / (m / 1e3) / 1e9})
     tot_fl = sum(o["flops"] for o in out)
     tot_ms = sum(o["ms"] for o in out)

@@ -87,6 +87,7 @@ def lib():
         "cq_mat_mult": [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int],
         "cq_mat_mult_host": [c_void_p, c_int, c_int, c_int, c_int, P(c_double), P(c_double), P(c_double), c_int],
         "cq_product_work": [c_void_p, c_int, c_int, c_int, c_int, P(c_int64), P(c_int64)],
+        "cq_product_tuning": [c_void_p, c_int, c_int, c_int, c_int, P(c_int), P(ctypes.c_float)],
         "cq_matrix_sum": [c_void_p, c_int, c_void_p, c_double, c_int, c_void_p, c_double],
         "cq_matrix_transpose": [c_void_p, c_int, c_void_p, c_void_p],
         "cq_matrix_trace": [c_void_p, c_int, c_void_p, P(c_double)],
@@ -223,6 +224,13 @@ class System:
         t, f = c_int64(), c_int64()
         check(lib().cq_product_work(self._h, mult_type, ra, rb, rc, ctypes.byref(t), ctypes.byref(f)))
         return t.value, f.value
+
+    def product_tuning(self, mult_type, ra, rb, rc):
+        """(variant chosen by the autotuner or -1, {variant: timed ms}) of one product."""
+        v = c_int()
+        ms = (ctypes.c_float * 4)()
+        check(lib().cq_product_tuning(self._h, mult_type, ra, rb, rc, ctypes.byref(v), ms))
+        return v.value, {i: ms[i] for i in range(4) if ms[i] > 0}
 
     def matrix_sum(self, ra, a, alpha, rb, b, beta):
         check(lib().cq_matrix_sum(self._h, ra, _ptr(a), float(alpha), rb, _ptr(b), float(beta)))

@@ -216,6 +216,15 @@ int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64
   });
 }
 
+int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int* variant, float* ms) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, ra); check_range(sys, rb); check_range(sys, rc);
+    ProductPlan& P = get_plan(sys->S, mult_type, ra, rb, rc);
+    if (variant) *variant = P.tuned;
+    if (ms) for (int v = 0; v < 4; ++v) ms[v] = P.tune_ms[v];
+  });
+}
+
 int cq_matrix_sum(cq_system* sys, int ra, double* a_dev, double alpha, int rb, const double* b_dev, double beta) {
   return guarded([&] {
     check_sys(sys); check_range(sys, ra); check_range(sys, rb);

@@ -138,8 +138,7 @@ void LNVSolver::purify(int sweeps) {
 
 void LNVSolver::msum(double alpha, DMat& A, double beta, const DMat& B) {
   if (A.rng == B.rng) {
-    dev_scale(S, A.p, A.n, alpha);
-    dev_axpy(S, A.p, A.n, beta, B.p);
+    dev_axpby(S, A.p, A.n, alpha, beta, B.p);
   } else {
     dev_matrix_add(S, R[A.rng], A.p, alpha, R[B.rng], B.p, beta);
   }

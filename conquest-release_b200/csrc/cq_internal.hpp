@@ -302,6 +302,8 @@ void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a,
 // algebra.cu
 void dev_scale(System& S, double* a, int64_t n, double alpha);
 void dev_axpy(System& S, double* a, int64_t n, double beta, const double* b);
+// a = fl(alpha*a) + fl(beta*b) elementwise: dev_scale then dev_axpy in one pass, same bits
+void dev_axpby(System& S, double* a, int64_t n, double alpha, double beta, const double* b);
 void dev_copy(System& S, double* dst, const double* src, int64_t n);
 void dev_matrix_add(System& S, int ra, double* a, double alpha, int rb, const double* b, double beta);
 void dev_transpose(System& S, int r, const double* a, double* at);

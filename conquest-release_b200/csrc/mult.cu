@@ -450,33 +450,36 @@ static void launch_variant(System& S, ProductPlan& P, const MultArgs& M, int var
   CQ_CUDA(cudaGetLastError());
 }
 
-// Autotuner: on the first call of a product, time each candidate kernel (one warm launch, then
-// one launch between CUDA events on the system's stream) and keep the fastest for the plan.  The
-// candidates give identical bits and each fully overwrites the output, so tuning changes speed
-// only; the last timed launch leaves the correct result.
+// Autotuner: on the first call of a product, time the candidate kernels (one warm launch each,
+// then three rounds in which every candidate runs once between CUDA events on the system's
+// stream; a candidate's time is its fastest round) and keep the fastest for the plan, the
+// warp-staged kernel unless another one is at least 5 % faster.  The candidates give identical
+// bits and each fully overwrites the output, so tuning changes speed only; the last timed launch
+// leaves the correct result.
 static int tuned_variant(System& S, ProductPlan& P, const MultArgs& M, int exact) {
   if (P.tuned >= 0) return P.tuned;
-  static const int kCands[] = {1, 3};
+  static const int kCands[] = {3, 1};
   cudaEvent_t e0, e1;
   CQ_CUDA(cudaEventCreate(&e0));
   CQ_CUDA(cudaEventCreate(&e1));
-  float best = 1e30f;
-  int pick = 3;
-  for (int v : kCands) {
-    launch_variant(S, P, M, v, exact, true);
-    CQ_CUDA(cudaEventRecord(e0, S.stream));
-    launch_variant(S, P, M, v, exact, true);
-    CQ_CUDA(cudaEventRecord(e1, S.stream));
-    CQ_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    CQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    P.tune_ms[v] = ms;
-    if (ms < best) { best = ms; pick = v; }
-  }
+  float best[2] = {1e30f, 1e30f};
+  for (int c = 0; c < 2; ++c) launch_variant(S, P, M, kCands[c], exact, true);
+  for (int round = 0; round < 3; ++round)
+    for (int c = 0; c < 2; ++c) {
+      CQ_CUDA(cudaEventRecord(e0, S.stream));
+      launch_variant(S, P, M, kCands[c], exact, true);
+      CQ_CUDA(cudaEventRecord(e1, S.stream));
+      CQ_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      best[c] = std::min(best[c], ms);
+    }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  P.tuned = pick;
-  return pick;
+  P.tune_ms[3] = best[0];
+  P.tune_ms[1] = best[1];
+  P.tuned = best[1] < 0.95f * best[0] ? 1 : 3;
+  return P.tuned;
 }
 
 void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, double* c, int exact) {

@@ -114,6 +114,10 @@ int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, doub
 /* Algorithmic work of one product: (k,i,j) triples with a stored result and 2*sum nd^3 flops. */
 int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* triples, int64_t* flops);
 
+/* Autotuner record of one product: the FP64 kernel variant it chose (-1 before the product's
+ * first autotuned call) and the timed milliseconds of each candidate variant (ms[4], 0 = not timed). */
+int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int* variant, float* ms);
+
 /*
  * Drop-in kernel pair (plugin surface of multiply_kernel_<MULT_KERN>.f90):
  * the argument lists of m_kern_max / m_kern_min
