@@ -81,7 +81,9 @@ void LNVSolver::product(const DMat& A, const DMat& B, DMat& C, MultId id) {
 }
 
 void LNVSolver::mult_dispatch(ProductPlan& P, double* a, const double* b, double* c) {
-  if (use_mixed) {
+  // Split precision only where it pays: a 16 x 16 tensor-core tile holds one padded block, so
+  // blocks of 8 x 8 or less (SZ, 4 x 4) run faster as FP64 products, which the phase keeps.
+  if (use_mixed && S.max_nsf > 8) {
     stats.n_products_mixed++;
     stats.flops_mixed += P.flops;
     mat_mult_mixed(S, P.mult_type, P.ra, P.rb, P.rc, a, b, c);

@@ -258,6 +258,7 @@ struct System {
   std::map<std::pair<int, int>, FragBuf> frags;   // (range, slot) fragment buffers of the mixed products
   cudaStream_t stream = nullptr;  // the stream all work of the system is enqueued on
   int uniform_nsf = 0;            // block size when every atom has the same one, else 0
+  int max_nsf = 0;                // largest block size
   DevBuf<double> red_scratch;     // scratch of the min/max reductions
   DevBuf<uint64_t> acc_part;      // 192-bit partials of the exact sums
   DevBuf<int> acc_flags;          // largest exponent, non-finite flag

@@ -437,6 +437,8 @@ void upload_geometry(System& S) {
   int u = g.nsf.empty() ? 0 : g.nsf[0];
   for (int v : g.nsf) if (v != u) { u = 0; break; }
   S.uniform_nsf = u;
+  S.max_nsf = 0;
+  for (int v : g.nsf) S.max_nsf = std::max(S.max_nsf, v);
 }
 
 void build_range_index(System& S, RangeIndex& R) {
