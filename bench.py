@@ -485,7 +485,8 @@ def serve_main(args):
         fp, t_fp = run_server(cq_b200, reqs, 1, False)
         mx, t_mx = run_server(cq_b200, reqs, args.slots, True, rate=rate, seed=11)
     bad = [r for r in fp + mx if r["status"] != 0]
-    err = max(abs(a["energy"] - b["energy"]) / a["n_atoms"] for a, b in zip(fp, mx))
+    ok = [(a, b) for a, b in zip(fp, mx) if a["status"] == 0 and b["status"] == 0 and a["converged"] and b["converged"]]
+    err = max([abs(a["energy"] - b["energy"]) / a["n_atoms"] for a, b in ok], default=None)
     lat = np.array([r["latency"] for r in mx]) * 1e3
     atoms = sum(r["n"] for r in reqs)
     flops_fp64 = sum(r["flops"] for r in fp)
@@ -504,6 +505,11 @@ def serve_main(args):
         "speedup_vs_fp64_path": t_fp / t_mx,
         "max_energy_error_per_atom": err,
         "failed": len(bad), "converged": sum(r["converged"] for r in mx),
+        "failures": [{"n_atoms": r["n_atoms"], "mixed": r["mixed"], "message": r["message"]} for r in bad][:8],
+        "per_request": [{"n": a["n_atoms"], "nsf": q["nsf"], "fp64_s": a["t_done"] - a["t_admit"],
+                         "mixed_s": b["t_done"] - b["t_admit"], "conv": [a["converged"], b["converged"]],
+                         "dE_per_atom": (b["energy"] - a["energy"]) / a["n_atoms"]}
+                        for a, b, q in zip(fp, mx, reqs)],
         "bytes_peak_max": max(r["bytes_peak"] for r in mx),
         "clocks": clk.summary(),
     }

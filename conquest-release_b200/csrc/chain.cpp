@@ -157,10 +157,11 @@ double LNVSolver::ptrace(const DMat& A, const DMat& B) {
 // Several matrix_product_trace values computed back to back and read with one host wait; the
 // values (and the reduction log) are those of the same ptrace calls in this order.
 void LNVSolver::ptraces(std::initializer_list<std::pair<const DMat*, const DMat*>> ops, double* out) {
-  const double* xs[32];
-  const double* ys[32];
-  int64_t ns[32];
+  const double* xs[32] = {};
+  const double* ys[32] = {};
+  int64_t ns[32] = {};
   int k = 0;
+  CQ_CHECK(ops.size() <= 32, CQ_ERR_ARG, "at most 32 traces per batch");
   for (auto& o : ops) {
     CQ_CHECK(o.first->rng == o.second->rng, CQ_ERR_STATE, "matrix_product_trace needs equal ranges");
     xs[k] = o.first->p; ys[k] = o.second->p; ns[k] = o.first->n;
@@ -595,6 +596,8 @@ int LNVSolver::early_dm(int ndone, bool& inflex) {
     msum(0.0, search, -1.0, SM3);
     if (prm.vary_mu) project_search(search, SM3, Sphi, mtemp);
     double g0 = gnorm(M3, SM3);
+    CQ_CHECK(std::isfinite(g0) && std::isfinite(energy0), CQ_ERR_NOT_CONVERGED,
+             "earlyDM: the residual or the energy is not finite");
     stats.early_iters++;
     stats.last_energy = energy0;
     stats.last_residual = g0;
@@ -670,16 +673,17 @@ int LNVSolver::late_dm(int ndone, bool& done, double& deltaE) {
     std::fill(Aij.begin(), Aij.end(), 0.0);
     {
       // the pul_mx^2 traces Tr(G_j SG_i), in the reference's loop order, read with one wait
-      const double* xs[32];
-      const double* ys[32];
-      int64_t ns[32];
-      double v[32];
+      const int nt = pul_mx * pul_mx;
+      std::vector<const double*> xs(nt), ys(nt);
+      std::vector<int64_t> ns(nt);
+      std::vector<double> v(nt);
       int k = 0;
       for (int i = 0; i < pul_mx; ++i)
         for (int j = 0; j < pul_mx; ++j) { xs[k] = Gst[j].p; ys[k] = SGst[i].p; ns[k] = Gst[j].n; ++k; }
       stats.n_reductions += k;
-      dev_dots(S, k, xs, ys, ns, v);
-      if (rlog_on) rlog.insert(rlog.end(), v, v + k);
+      for (int k0 = 0; k0 < nt; k0 += 32)     // dev_dots reads at most 32 sums per wait
+        dev_dots(S, std::min(32, nt - k0), xs.data() + k0, ys.data() + k0, ns.data() + k0, v.data() + k0);
+      if (rlog_on) rlog.insert(rlog.end(), v.begin(), v.end());
       k = 0;
       for (int i = 0; i < pul_mx; ++i)
         for (int j = 0; j < pul_mx; ++j) Aij[j + npul * i] = 2.0 * v[k++];
@@ -694,6 +698,8 @@ int LNVSolver::late_dm(int ndone, bool& done, double& deltaE) {
     if (prm.vary_mu) project_gradient(M3, SM3, Sphi, mtemp);
     deltaE = energy1 - energy0;
     double g1 = gnorm(M3, SM3);
+    CQ_CHECK(std::isfinite(g1) && std::isfinite(energy1), CQ_ERR_NOT_CONVERGED,
+             "lateDM: the residual or the energy is not finite");
     stats.late_iters++;
     stats.last_energy = energy1;
     stats.last_residual = g1;
@@ -761,7 +767,8 @@ bool sym_inverse_bk(double* A, int n) {
     double colmax = 0.0;
     for (int i = 0; i < k; ++i) if (std::fabs(a(i, k)) > colmax) { colmax = std::fabs(a(i, k)); imax = i; }
     int kp;
-    if (std::max(absakk, colmax) == 0.0) return false;
+    // a zero or NaN pivot column: singular (dsytf2 sets INFO and leaves the column)
+    if (std::max(absakk, colmax) == 0.0 || std::isnan(absakk)) return false;
     if (absakk >= alpha * colmax) kp = k;
     else {
       double rowmax = 0.0;

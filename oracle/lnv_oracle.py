@@ -61,7 +61,7 @@ def bk_inverse(A):
         for i in range(k):
             if abs(a[i][k]) > colmax:
                 colmax = abs(a[i][k]); imax = i
-        if max(absakk, colmax) == 0.0:
+        if max(absakk, colmax) == 0.0 or math.isnan(absakk):
             return None
         if absakk >= alpha * colmax:
             kp = k

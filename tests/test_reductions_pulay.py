@@ -56,3 +56,17 @@ def test_exact_sum_is_order_independent():
     # exact cancellation inside the 150-bit window, truncation below it (by design)
     assert o.exact_dot(np.array([1e30, -1e30, 3.0])) == 3.0
     assert o.exact_dot(np.array([1e300, -1e300, 3.0])) == 0.0
+
+
+def test_pulay_nan_matrix_is_singular():
+    """A NaN pivot makes the Pulay matrix singular (dsytf2's INFO), as in the oracle: the mixing then
+    keeps the newest iterate instead of reading outside the matrix."""
+    import math
+    import cq_b200
+    from lnv_oracle import bk_inverse
+    A = np.eye(3)
+    A[0, 0] = float("nan")
+    al = cq_b200.pulay_alphas(2, A, 3, 5)
+    assert al[1] == 1.0 and al[0] == 0.0 and al[2] == 0.0
+    assert bk_inverse([list(r) for r in A]) is None
+    assert not math.isnan(al.sum())
