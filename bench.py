@@ -259,6 +259,8 @@ def main():
     ap.add_argument("--nmax", type=int, default=1000)
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--rate", type=float, default=200.0)
+    ap.add_argument("--tol", type=float, default=None, help="batch/serve: residual tolerance of both arms")
+    ap.add_argument("--max-outer", type=int, default=None, help="batch/serve: FindMinDM pass limit per request")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.workload in ("mult216", "mult512", "mult4096") and args.impl == "ours":
@@ -425,6 +427,7 @@ SERVE_RANGES = (10.0, 12.0, 16.0, 10.0)   # S, H, L, T (bohr), as the 512-atom w
 # residual at which both arms stop: at the default 1e-7 two FP64 solves of one problem from different
 # starting points differ by ~1e-7 Ha/atom, so the 1e-8 Ha/atom comparison needs a tighter stop
 SERVE_TOL = 1e-9
+SERVE_MAX_OUTER = 4        # FindMinDM passes per request (a stalled residual stops there)
 
 
 def request_set(n_req, nmin, nmax, seed):
@@ -449,7 +452,8 @@ def request_set(n_req, nmin, nmax, seed):
 
 def run_server(cq_b200, reqs, n_slots, mixed, rate=None, seed=0):
     """Submit the requests (all at once, or as a Poisson stream of `rate` per second) and wait for all."""
-    srv = cq_b200.Server(n_slots=n_slots, hbm_budget=int(0.8 * torch_total_mem()), tolerance=SERVE_TOL)
+    srv = cq_b200.Server(n_slots=n_slots, hbm_budget=int(0.8 * torch_total_mem()), tolerance=SERVE_TOL,
+                         max_outer=SERVE_MAX_OUTER)
     t_arr = np.zeros(len(reqs))
     if rate:
         t_arr = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, size=len(reqs)))
@@ -477,6 +481,11 @@ def serve_main(args):
     import torch
     import cq_b200
     torch.cuda.set_device(0)
+    global SERVE_TOL, SERVE_MAX_OUTER
+    if args.tol is not None:
+        SERVE_TOL = args.tol
+    if args.max_outer is not None:
+        SERVE_MAX_OUTER = args.max_outer
     reqs = request_set(args.requests, args.nmin, args.nmax, seed=7)
     rate = args.rate if args.workload == "serve" else None
     warm = request_set(2, 64, 64, seed=99)
@@ -497,7 +506,7 @@ def serve_main(args):
         "config": {"workload": "lnv_%s_si_mixed" % args.workload, "requests": len(reqs),
                    "atoms": [args.nmin, args.nmax], "atoms_total": atoms, "blocks": "4x4 and 13x13",
                    "ranges_bohr": dict(zip("SHLT", SERVE_RANGES)), "arrival_rate_per_s": rate,
-                   "slots": args.slots, "tolerance": SERVE_TOL},
+                   "slots": args.slots, "tolerance": SERVE_TOL, "max_outer": SERVE_MAX_OUTER},
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
         "fp64_path": {"value": len(reqs) / t_fp, "unit": "solves/s", "slots": 1,
                       "latency_ms_p50": float(np.percentile([r["latency"] * 1e3 for r in fp], 50)),

@@ -31,14 +31,16 @@ class LNVParams(ctypes.Structure):
     _fields_ = [("n_L_iterations", c_int), ("tolerance", c_double), ("maxpulay", c_int), ("minpulaystep", c_double),
                 ("maxpulaystep", c_double), ("lintol", c_double), ("global_tolerance", c_int), ("vary_mu", c_int),
                 ("invs_max_steps", c_int), ("invs_delta_tol", c_double), ("invs_tol", c_double), ("exact", c_int),
-                ("max_outer", c_int), ("mixed", c_int), ("mixed_tolerance", c_double), ("fp64_mcw_sweeps", c_int)]
+                ("max_outer", c_int), ("mixed", c_int), ("mixed_tolerance", c_double), ("fp64_mcw_sweeps", c_int),
+                ("graphs", c_int)]
 
 
 class LNVResult(ctypes.Structure):
     """cq_lnv_result (include/cq_b200.h)."""
     _fields_ = [("energy", c_double), ("electrons", c_double), ("residual", c_double), ("invs_omega", c_double),
                 ("mcw_sweeps", c_int), ("early_iters", c_int), ("late_iters", c_int), ("ne_corrections", c_int),
-                ("inflexions", c_int), ("converged", c_int), ("outer_iters", c_int), ("n_products", c_int64),
+                ("inflexions", c_int), ("converged", c_int), ("outer_iters", c_int), ("graph_launches", c_int64),
+                ("n_products", c_int64),
                 ("flops", c_int64),
                 ("n_products_mixed", c_int64), ("flops_mixed", c_int64)]
 

@@ -353,16 +353,26 @@ static double exact_sum(System& S, const double* x, const double* y, int64_t n) 
   return exact_sum_value(w);
 }
 
-void dev_dots(System& S, int count, const double* const* x, const double* const* y, const int64_t* n, double* out) {
+void dev_dots_enqueue(System& S, int count, const double* const* x, const double* const* y, const int64_t* n) {
   CQ_CHECK(count >= 0 && count <= kSumSlots, CQ_ERR_ARG, "too many sums in one batch");
   if (count == 0) return;
   acc_scratch(S);
+  static_assert(4 * kSumSlots <= kPinnedWords, "pinned result buffer too small");
+  if (!S.host_res) S.host_res = pinned_get();
   uint64_t* res = S.acc_part.p + 3 * kRedBlocks;
   for (int k = 0; k < count; ++k) exact_sum_enqueue(S, x[k], y[k], n[k], S.acc_flags.p + 2 * k, S.acc_part.p, res + 4 * k);
-  std::vector<uint64_t> w(4 * (size_t)count);
-  CQ_CUDA(cudaMemcpyAsync(w.data(), res, sizeof(uint64_t) * w.size(), cudaMemcpyDeviceToHost, S.stream));
+  CQ_CUDA(cudaMemcpyAsync(S.host_res, res, sizeof(uint64_t) * 4 * count, cudaMemcpyDeviceToHost, S.stream));
+}
+
+void dev_dots_fetch(System& S, int count, double* out) {
+  if (count == 0) return;
   host_wait(S);
-  for (int k = 0; k < count; ++k) out[k] = exact_sum_value(&w[4 * k]);
+  for (int k = 0; k < count; ++k) out[k] = exact_sum_value(&S.host_res[4 * k]);
+}
+
+void dev_dots(System& S, int count, const double* const* x, const double* const* y, const int64_t* n, double* out) {
+  dev_dots_enqueue(S, count, x, y, n);
+  dev_dots_fetch(S, count, out);
 }
 
 double dev_dot(System& S, const double* x, const double* y, int64_t n) { return exact_sum(S, x, y, n); }

@@ -42,6 +42,25 @@ System::~System() {
   // before they are released (on the stream recorded at their allocation)
   if (stream) cudaStreamSynchronize(stream);
   if (sync_ev) cudaEventDestroy(sync_ev);
+  if (host_res) pinned_put(host_res);
+}
+
+// Small pinned host buffers (exact-sum results) are kept in a process-wide free list: freeing
+// pinned memory can synchronise the device, which would stall the solves of other systems.
+static std::mutex g_pinned_mu;
+static std::vector<uint64_t*> g_pinned_free;
+uint64_t* pinned_get() {
+  {
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    if (!g_pinned_free.empty()) { uint64_t* p = g_pinned_free.back(); g_pinned_free.pop_back(); return p; }
+  }
+  uint64_t* p = nullptr;
+  CQ_CUDA(cudaMallocHost((void**)&p, kPinnedWords * sizeof(uint64_t)));
+  return p;
+}
+void pinned_put(uint64_t* p) {
+  std::lock_guard<std::mutex> lk(g_pinned_mu);
+  g_pinned_free.push_back(p);
 }
 
 void host_wait(System& S) {

@@ -28,6 +28,7 @@ static void fill_result(const LNVStats& st, cq_lnv_result* r) {
   r->inflexions = st.inflexions;
   r->converged = st.converged;
   r->outer_iters = st.outer_iters;
+  r->graph_launches = st.graph_launches;
   r->n_products = st.n_products;
   r->flops = st.flops;
   r->n_products_mixed = st.n_products_mixed;
@@ -65,6 +66,7 @@ int cq_lnv_params_default(cq_lnv_params* p) {
   p->mixed = 0;
   p->mixed_tolerance = 1.0e-5;
   p->fp64_mcw_sweeps = 0;
+  p->graphs = 1;
   return CQ_OK;
 }
 

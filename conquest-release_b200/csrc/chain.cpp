@@ -216,59 +216,130 @@ DMat LNVSolver::own(int rng) {
 }
 
 // ---- LNV_matrix_multiply (doK, doM3, dophi, doE) ---------------------------
-void LNVSolver::lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim, double* electrons, double* energy) {
+// The temporaries of one call live in a workspace owned by the solver (allocate_temp_matrix
+// hands out zeroed matrices; every one of them except A is fully overwritten by a product or a
+// transpose before it is read, so only A is cleared), which keeps the device addresses of a call
+// fixed: the call can then be captured once in a CUDA graph and replayed.
+void LNVSolver::ensure_workspace() {
+  if (ws_ready) return;
+  wLH = own(RLH); wHL = own(RLH); wHLS = own(RLSL); wSLH = own(RLSL); wA = own(RLSL);
+  wBm = own(RL); wCm = own(RL); wSLS = own(RSLS); wSLSLS = own(RL); wLSLSL = own(RH);
+  ws_ready = true;
+}
+
+// Everything of one call up to the traces, enqueued on S.stream with no host synchronisation;
+// returns the number of traces enqueued (their values: dev_dots_fetch).
+int LNVSolver::lnv_body(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim) {
   product(L, Smat, LS, L_S_LS);
   transpose(LS, SL);
-  DMat HLS, SLH, Bm, Cm, SLS, SLSLS, LSL, LSLSL;
   if (doM3) {
-    DMat LH = temp(RLH), HL = temp(RLH);
-    product(L, Hmat, LH, L_H_LH);
-    transpose(LH, HL);
-    HLS = temp(RLSL); SLH = temp(RLSL);
-    DMat A = temp(RLSL);
-    Bm = temp(RL); Cm = temp(RL);
-    product(HL, Smat, HLS, HL_S_LSL);
-    product(HL, Smat, HLS, HL_S_LSL);   // computed twice in the reference (mult_module.f90:1609, 1615)
-    transpose(HLS, SLH);
-    msum(0.0, A, 2.0, HLS);
-    msum(1.0, A, 1.0, SLH);
-    product(A, SL, Bm, HLS_LS_L);
-    transpose(Bm, Cm);
+    product(L, Hmat, wLH, L_H_LH);
+    transpose(wLH, wHL);
+    CQ_CUDA(cudaMemsetAsync(wA.p, 0, sizeof(double) * std::max<int64_t>(wA.n, 1), S.stream));
+    product(wHL, Smat, wHLS, HL_S_LSL);
+    product(wHL, Smat, wHLS, HL_S_LSL);   // computed twice in the reference (mult_module.f90:1609, 1615)
+    transpose(wHLS, wSLH);
+    msum(0.0, wA, 2.0, wHLS);
+    msum(1.0, wA, 1.0, wSLH);
+    product(wA, SL, wBm, HLS_LS_L);
+    transpose(wBm, wCm);
   }
   if (dophi) {
-    SLS = temp(RSLS); SLSLS = temp(RL);
-    product(SL, Smat, SLS, SL_S_SLS);
-    product(SLS, SL, SLSLS, SLS_LS_L);
+    product(SL, Smat, wSLS, SL_S_SLS);
+    product(wSLS, SL, wSLSLS, SLS_LS_L);
   }
   if (doK || doE) {
-    LSL = temp(RLSL); LSLSL = temp(RH);
+    DMat& LSL = wA;                      // A is dead here; LSL takes its matrix
     product(LS, L, LSL, LS_L_LSL);
-    product(LSL, LS, LSLSL, LSL_SL_H);
+    product(LSL, LS, wLSLSL, LSL_SL_H);
     msum(0.0, K, 3.0, LSL);
-    msum(1.0, K, -2.0, LSLSL);
+    msum(1.0, K, -2.0, wLSLSL);
   }
   if (doM3) {
-    msum(0.0, *M3, 3.0, HLS);
-    msum(1.0, *M3, 3.0, SLH);
-    msum(1.0, *M3, -1.0, Bm);
-    msum(1.0, *M3, -1.0, Cm);
+    msum(0.0, *M3, 3.0, wHLS);
+    msum(1.0, *M3, 3.0, wSLH);
+    msum(1.0, *M3, -1.0, wBm);
+    msum(1.0, *M3, -1.0, wCm);
   }
-  // Tr(HK), Tr(L SLS), Tr(L SLSLS): enqueued back to back (before phi is overwritten) and read
-  // together; the reference computes them in this order (mult_module.f90:1700-1800)
-  double t[3];
-  if (dophi) msum(0.0, *phim, 1.0, SLS);
-  if (doE && dophi) {
-    ptraces({{&Hmat, &K}, {&L, phim}, {&L, &SLSLS}}, t);
-  } else if (doE) {
-    ptraces({{&Hmat, &K}}, t);
-  } else if (dophi) {
-    ptraces({{&L, phim}, {&L, &SLSLS}}, t + 1);
-  }
-  if (doE) *energy = t[0];
+  if (dophi) msum(0.0, *phim, 1.0, wSLS);
+  // Tr(HK), Tr(L SLS), Tr(L SLSLS), enqueued before phi is overwritten, in the reference's order
+  // (mult_module.f90:1700-1800)
+  const double* xs[3];
+  const double* ys[3];
+  int64_t ns[3];
+  int k = 0;
+  if (doE) { xs[k] = Hmat.p; ys[k] = K.p; ns[k] = Hmat.n; ++k; }
   if (dophi) {
-    *electrons = 3.0 * t[1] - 2.0 * t[2];
-    msum(6.0, *phim, -6.0, SLSLS);
+    xs[k] = L.p; ys[k] = phim->p; ns[k] = L.n; ++k;
+    xs[k] = L.p; ys[k] = wSLSLS.p; ns[k] = L.n; ++k;
   }
+  dev_dots_enqueue(S, k, xs, ys, ns);
+  if (dophi) msum(6.0, *phim, -6.0, wSLSLS);
+  return k;
+}
+
+LNVSolver::~LNVSolver() {
+  for (auto& g : graphs_) if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+}
+
+// One LNV_matrix_multiply call.  With prm.graphs, the first call with a given set of operands runs
+// directly (it builds and tunes the products' plans and allocates their buffers), the second is
+// captured into a CUDA graph, and later ones replay that graph: one launch instead of ~60.
+void LNVSolver::lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim, double* electrons, double* energy) {
+  ensure_workspace();
+  int nsum = 0;
+  auto body = [&] { nsum = lnv_body(doK, doM3, dophi, doE, M3, phim); };
+  if (!prm.graphs || S.prof.on) {
+    body();
+  } else {
+    const std::vector<uintptr_t> key = {(uintptr_t)(doK | doM3 << 1 | dophi << 2 | doE << 3 | use_mixed << 4),
+                                        (uintptr_t)(M3 ? M3->p : nullptr), (uintptr_t)(phim ? phim->p : nullptr)};
+    auto it = graphs_.find(key);
+    if (it != graphs_.end()) {
+      LnvGraph& g = it->second;
+      CQ_CUDA(cudaGraphLaunch(g.exec, S.stream));
+      S.launches += g.launches;
+      stats.n_products += g.products; stats.flops += g.flops;
+      stats.n_products_mixed += g.products_mixed; stats.flops_mixed += g.flops_mixed;
+      nsum = g.nsum;
+      stats.graph_launches++;
+    } else if (seen_[key]++ == 0) {
+      body();
+    } else {
+      if (graphs_.size() >= 32) {        // bound the cache
+        for (auto& g : graphs_) if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+        graphs_.clear();
+      }
+      const int64_t l0 = S.launches, p0 = stats.n_products, f0 = stats.flops, pm0 = stats.n_products_mixed,
+                    fm0 = stats.flops_mixed;
+      CQ_CUDA(cudaStreamBeginCapture(S.stream, cudaStreamCaptureModeThreadLocal));
+      cudaGraph_t graph = nullptr;
+      try {
+        body();
+      } catch (...) {
+        cudaStreamEndCapture(S.stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+      }
+      CQ_CUDA(cudaStreamEndCapture(S.stream, &graph));
+      LnvGraph g;
+      cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      CQ_CUDA(e);
+      g.launches = S.launches - l0; g.products = stats.n_products - p0; g.flops = stats.flops - f0;
+      g.products_mixed = stats.n_products_mixed - pm0; g.flops_mixed = stats.flops_mixed - fm0;
+      g.nsum = nsum;
+      CQ_CUDA(cudaGraphLaunch(g.exec, S.stream));
+      graphs_[key] = g;
+      stats.graph_launches++;
+    }
+  }
+  double t[3] = {0, 0, 0};
+  dev_dots_fetch(S, nsum, t);
+  stats.n_reductions += nsum;
+  if (rlog_on) rlog.insert(rlog.end(), t, t + nsum);
+  if (doE) *energy = t[0];
+  if (dophi) *electrons = 3.0 * t[doE ? 1 : 0] - 2.0 * t[doE ? 2 : 1];
   stats.n_lnv++;
 }
 
@@ -384,7 +455,9 @@ void LNVSolver::init_mcw() {
 
 void LNVSolver::mcw_mm_nonds(DMat& RhoNew, double& energy, double& c) {
   product(L, Smat, LS, L_S_LS);
-  DMat LSL = temp(RLSL), LSLSL = temp(RL), top = temp(RS), bottom = temp(RS);
+  ensure_workspace();
+  DMat& LSL = wA;                        // the LNV workspace's LSL-range matrix, free outside lnv()
+  DMat LSLSL = temp(RL), top = temp(RS), bottom = temp(RS);
   product(LS, L, LSL, LS_L_LSL);
   product(LSL, LS, LSLSL, HLS_LS_L);
   msum(0.0, top, 1.0, LSL);

@@ -38,6 +38,7 @@ struct LNVStats {
   int64_t n_products = 0, flops = 0, n_reductions = 0, n_lnv = 0, n_products_mixed = 0, flops_mixed = 0;
   int mcw_sweeps = 0, early_iters = 0, late_iters = 0, ne_corrections = 0, inflexions = 0, converged = 0;
   int outer_iters = 0;
+  int64_t graph_launches = 0;     // LNV calls run as CUDA graph launches
   double energy = 0, electrons = 0, last_energy = 0, last_residual = 0, invs_omega = 0;
   double mubar = 0, lambda = 0, hmin = 0, hmax = 0;
 };
@@ -52,6 +53,7 @@ class LNVSolver {
   static const Mult kMults[];
 
   LNVSolver(System& sys, const int ranges[NR], double ne_spin, const cq_lnv_params& p);
+  ~LNVSolver();
 
   System& S;
   cq_lnv_params prm;
@@ -78,6 +80,18 @@ class LNVSolver {
   void lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim, double* electrons, double* energy);
 
  private:
+  // workspace of lnv(): fixed addresses so a call can be captured in a CUDA graph
+  DMat wLH, wHL, wHLS, wSLH, wA, wBm, wCm, wSLS, wSLSLS, wLSLSL;
+  bool ws_ready = false;
+  void ensure_workspace();
+  int lnv_body(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim);
+  struct LnvGraph {
+    cudaGraphExec_t exec = nullptr;
+    int64_t launches = 0, products = 0, flops = 0, products_mixed = 0, flops_mixed = 0;
+    int nsum = 0;
+  };
+  std::map<std::vector<uintptr_t>, LnvGraph> graphs_;
+  std::map<std::vector<uintptr_t>, int> seen_;
   std::vector<DevBuf<double>> owned_;
   std::vector<DevBuf<double>> pool_;
   std::map<int, std::vector<double*>> free_;

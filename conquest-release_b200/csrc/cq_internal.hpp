@@ -264,6 +264,7 @@ struct System {
   DevBuf<int> acc_flags;          // largest exponent, non-finite flag
   DevBuf<int> diag_off;           // first onsite-diagonal slot of each primary atom
   DevBuf<double> diag_buf;        // gathered onsite diagonal (exact trace)
+  uint64_t* host_res = nullptr;   // pinned host copy of the exact-sum results (4 words per sum)
   int64_t launches = 0;           // kernels launched by this system (all kinds)
   int mult_variant = -1;          // 4x4 FP64 product kernel: -1 = chosen per product by the autotuner,
                                   // 0 = one lane per element, 1 = one thread per block,
@@ -277,6 +278,9 @@ struct System {
 
 void init_device_pool();          // once per device: cache freed pool memory in the process
 void host_wait(System& S);        // wait for all work enqueued on S.stream
+constexpr int kPinnedWords = 4 * 32;
+uint64_t* pinned_get();           // kPinnedWords of pinned host memory from a process-wide free list
+void pinned_put(uint64_t* p);
 
 // index.cu
 void upload_geometry(System& S);
@@ -312,6 +316,10 @@ double dev_dot(System& S, const double* x, const double* y, int64_t n);
 // up to 32 exact dot products (y[k] may be null: plain sums), computed back to back and read
 // with one host synchronisation
 void dev_dots(System& S, int count, const double* const* x, const double* const* y, const int64_t* n, double* out);
+// the same in two halves: enqueue the sums and the copy of their results to pinned host memory
+// (no host synchronisation: can be captured in a CUDA graph), then wait and decode
+void dev_dots_enqueue(System& S, int count, const double* const* x, const double* const* y, const int64_t* n);
+void dev_dots_fetch(System& S, int count, double* out);
 double dev_trace(System& S, int r, const double* a);
 void dev_h_limits(System& S, int r, const double* h, double* hmin, double* hmax);
 

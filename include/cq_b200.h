@@ -214,6 +214,8 @@ typedef struct {
                               to `tolerance`; Hotelling, traces, line search and Pulay stay FP64 */
   double mixed_tolerance;  /* residual at which the split-precision phase hands over to FP64 */
   int fp64_mcw_sweeps;     /* FP64 McWeeny purification sweeps of L between the two phases (0) */
+  int graphs;              /* 1: each LNV_matrix_multiply call is captured once in a CUDA graph and replayed
+                              (same results; default 1) */
 } cq_lnv_params;
 
 typedef struct {
@@ -223,6 +225,7 @@ typedef struct {
   double invs_omega;       /* Hotelling residual of T = S^-1 */
   int mcw_sweeps, early_iters, late_iters, ne_corrections, inflexions, converged;
   int outer_iters;         /* FindMinDM passes (early + late) run */
+  int64_t graph_launches;  /* LNV_matrix_multiply calls replayed from a CUDA graph */
   int64_t n_products;      /* block-sparse products executed */
   int64_t flops;           /* algorithmic flops of those products (2 sum nd_i nd_j nd_k) */
   int64_t n_products_mixed;/* of which with split-precision tensor-core arithmetic */

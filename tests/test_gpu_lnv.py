@@ -31,7 +31,7 @@ def _setup(coords, cell, nsf, ne_spin, rs=10.0, rh=12.0, rl=16.0, rt=10.0, **par
     blH = bm.oracle_blocklist(o, ridx["H"], coords, cell)
     S, H = inputs.overlap_S(blS), inputs.hamiltonian_H(blH, seed=5)
     olnv = OracleLNV(o, ridx, S, H, ne_spin, float(np.sum(nsf)),
-                     Params(**{k: v for k, v in params.items() if k != "max_outer"}))
+                     Params(**{k: v for k, v in params.items() if k not in ("max_outer", "graphs")}))
     glnv = cq_b200.LNV(g, ridx, ne_spin, **params)
     return o, g, ridx, S, H, olnv, glnv
 
@@ -84,3 +84,21 @@ def test_periodic_matches_oracle_chain(case):
     assert abs(res["energy"] - gold["energy"]) <= 1e-10 * max(1.0, abs(gold["energy"]))
     assert abs(res["electrons"] - gold["electrons"]) <= 1e-10 * max(1.0, abs(gold["electrons"]))
     assert hashlib.sha256(np.ascontiguousarray(L, np.float64).tobytes()).hexdigest() == gold["L_sha256"]
+
+
+def test_graph_replay_matches_direct_launches():
+    """LNV_matrix_multiply calls replayed from CUDA graphs give the same bits as direct launches."""
+    gold = GOLDEN["cases"]["r8_9_10_8"]
+    coords, cell = inputs.diamond_si(2, sigma=0.1, seed=2)
+    n = len(coords)
+    out = []
+    for graphs in (0, 1):
+        o, g, ridx, S, H, olnv, glnv = _setup(coords, cell, np.full(n, 4), float(n), *gold["ranges"],
+                                              max_outer=gold["max_outer"], graphs=graphs)
+        res, L, K = glnv.solve_host(S, H, want_L=True)
+        out.append((res, L))
+    (r0, L0), (r1, L1) = out
+    assert r0["graph_launches"] == 0 and r1["graph_launches"] > 0
+    assert (r0["energy"], r0["electrons"], r0["n_products"]) == (r1["energy"], r1["electrons"], r1["n_products"])
+    assert np.array_equal(L0, L1)
+    assert hashlib.sha256(np.ascontiguousarray(L1, np.float64).tobytes()).hexdigest() == gold["L_sha256"]
