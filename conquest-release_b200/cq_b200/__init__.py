@@ -230,9 +230,9 @@ class System:
     def product_tuning(self, mult_type, ra, rb, rc):
         """(variant chosen by the autotuner or -1, {variant: timed ms}) of one product."""
         v = c_int()
-        ms = (ctypes.c_float * 4)()
+        ms = (ctypes.c_float * 5)()
         check(lib().cq_product_tuning(self._h, mult_type, ra, rb, rc, ctypes.byref(v), ms))
-        return v.value, {i: ms[i] for i in range(4) if ms[i] > 0}
+        return v.value, {i: ms[i] for i in range(5) if ms[i] > 0}
 
     def matrix_sum(self, ra, a, alpha, rb, b, beta):
         check(lib().cq_matrix_sum(self._h, ra, _ptr(a), float(alpha), rb, _ptr(b), float(beta)))

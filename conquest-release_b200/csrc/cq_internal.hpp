@@ -207,7 +207,7 @@ struct ProductPlan {
   DevBuf<int4> tiles;
   DevBuf<int> order;              // output blocks by descending pair count (warp-staged 4x4 kernel)
   int tuned = -1;                 // FP64 kernel variant chosen by the autotuner (-1: not tuned yet)
-  float tune_ms[4] = {0, 0, 0, 0};
+  float tune_ms[5] = {0, 0, 0, 0, 0};
 };
 
 // Split-precision tensor-core product: pair lists sorted by the first operand block,
@@ -269,7 +269,9 @@ struct System {
   int mult_variant = -1;          // 4x4 FP64 product kernel: -1 = chosen per product by the autotuner,
                                   // 0 = one lane per element, 1 = one thread per block,
                                   // 2 = one thread per block with the operand row staged in shared memory,
-                                  // 3 = one thread per block with warp-cooperative staging of the operand blocks
+                                  // 3 = one thread per block with warp-cooperative staging of the operand blocks;
+                                  // other block sizes: 0 = generic warp per block, 4 = warp per block with
+                                  // 4 x 2 register tiles per lane
   bool blocking_sync = false;     // host waits sleep on a blocking-sync event instead of spinning
   cudaEvent_t sync_ev = nullptr;
   ProductProfile prof;

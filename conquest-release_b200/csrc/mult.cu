@@ -336,6 +336,72 @@ __global__ void __launch_bounds__(128, 5) k_mult_nd4_warp(MultArgs M, const int*
   }
 }
 
+// Any block sizes up to 16 (DZP 13 x 13, mixed SZ/DZP): one warp per output block, each lane a
+// 4 x 2 register tile of the output block (rows 4rt..4rt+3, columns 2ct..2ct+1, lane = rt * nct + ct),
+// so per term of the inner sum a lane loads 4 + 2 operand values for 8 multiply-adds instead of
+// 2 per multiply-add.  The order of the terms of every element is unchanged.
+template <int TYPE, bool EXACT>
+__global__ void __launch_bounds__(256) k_mult_tile(MultArgs M) {
+  const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (q >= M.n_out) return;
+  const int ndi = M.prim_nsf[M.o_row[q]];
+  const int ndo = M.cover_nsf[M.o_cover[q]];     // type 1: nd_j ; type 2: nd_k
+  const int nct = (ndo + 1) >> 1, nrt = (ndi + 3) >> 2;
+  const int rt = lane / nct, ct = lane - rt * nct;
+  const bool live = rt < nrt;                       // lanes beyond the tiles only keep the warp together
+  int r[4], c[2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) r[i] = min(4 * rt + i, ndi - 1);     // clamped: in-bounds reads
+#pragma unroll
+  for (int j = 0; j < 2; ++j) c[j] = min(2 * ct + j, ndo - 1);
+  double acc[4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) { acc[i][0] = 0.0; acc[i][1] = 0.0; }
+  const int64_t p0 = M.ptr[q], p1 = M.ptr[q + 1];
+  if (live) {
+    for (int64_t t = p0; t < p1; ++t) {
+      const int2 pr = M.pairs[t];
+      const double* X = M.x + M.x_elem[pr.x];
+      const double* B = M.b + M.b_elem[pr.y];
+      if (TYPE == 1) {
+        const int ndk = M.cover_nsf[M.x_cover[pr.x]];
+        for (int n3 = 0; n3 < ndk; ++n3) {
+          double xv[4], bv[2];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) xv[i] = __ldg(X + r[i] + ndi * n3);
+#pragma unroll
+          for (int j = 0; j < 2; ++j) bv[j] = __ldg(B + n3 + ndk * c[j]);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) acc[i][j] = madd<EXACT>(acc[i][j], xv[i], bv[j]);
+        }
+      } else {
+        const int ndj = M.cover_nsf[M.b_cover[pr.y]];
+        for (int n2 = 0; n2 < ndj; ++n2) {
+          double xv[4], bv[2];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) xv[i] = __ldg(X + r[i] + ndi * n2);
+#pragma unroll
+          for (int j = 0; j < 2; ++j) bv[j] = __ldg(B + c[j] + ndo * n2);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) acc[i][j] = madd<EXACT>(acc[i][j], xv[i], bv[j]);
+        }
+      }
+    }
+    double* O = M.out + M.o_elem[q];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int n1 = 4 * rt + i, n2 = 2 * ct + j;
+        if (n1 < ndi && n2 < ndo) O[n1 + ndi * n2] = acc[i][j];
+      }
+  }
+}
+
 // One drop-in m_kern_max (type 1) / m_kern_min (type 2) call: output blocks with explicit
 // offsets, accumulated in place in the layouts mat_mult passes (type 1 reads the local
 // transpose a(n3 + nd3*n1); type 2 accumulates into it).  One warp per output block.
@@ -438,6 +504,13 @@ static void launch_variant(System& S, ProductPlan& P, const MultArgs& M, int var
     } else {
       if (exact) k_mult_nd4<2, true><<<grid, T, 0, st>>>(M); else k_mult_nd4<2, false><<<grid, T, 0, st>>>(M);
     }
+  } else if (variant == 4) {
+    int grid = (int)(((int64_t)M.n_out * 32 + T - 1) / T);
+    if (P.mult_type == 1) {
+      if (exact) k_mult_tile<1, true><<<grid, T, 0, st>>>(M); else k_mult_tile<1, false><<<grid, T, 0, st>>>(M);
+    } else {
+      if (exact) k_mult_tile<2, true><<<grid, T, 0, st>>>(M); else k_mult_tile<2, false><<<grid, T, 0, st>>>(M);
+    }
   } else {
     int grid = (int)(((int64_t)M.n_out * 32 + T - 1) / T);
     if (P.mult_type == 1) {
@@ -456,18 +529,19 @@ static void launch_variant(System& S, ProductPlan& P, const MultArgs& M, int var
 // warp-staged kernel unless another one is at least 5 % faster.  The candidates give identical
 // bits and each fully overwrites the output, so tuning changes speed only; the last timed launch
 // leaves the correct result.
-static int tuned_variant(System& S, ProductPlan& P, const MultArgs& M, int exact) {
+static int tuned_variant(System& S, ProductPlan& P, const MultArgs& M, int exact, bool nd4) {
   if (P.tuned >= 0) return P.tuned;
-  static const int kCands[] = {3, 1};
+  // candidates: the preferred kernel first, the alternative second
+  const int kCands[2] = {nd4 ? 3 : 4, nd4 ? 1 : 0};
   cudaEvent_t e0, e1;
   CQ_CUDA(cudaEventCreate(&e0));
   CQ_CUDA(cudaEventCreate(&e1));
   float best[2] = {1e30f, 1e30f};
-  for (int c = 0; c < 2; ++c) launch_variant(S, P, M, kCands[c], exact, true);
+  for (int c = 0; c < 2; ++c) launch_variant(S, P, M, kCands[c], exact, nd4);
   for (int round = 0; round < 3; ++round)
     for (int c = 0; c < 2; ++c) {
       CQ_CUDA(cudaEventRecord(e0, S.stream));
-      launch_variant(S, P, M, kCands[c], exact, true);
+      launch_variant(S, P, M, kCands[c], exact, nd4);
       CQ_CUDA(cudaEventRecord(e1, S.stream));
       CQ_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
@@ -476,9 +550,9 @@ static int tuned_variant(System& S, ProductPlan& P, const MultArgs& M, int exact
     }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  P.tune_ms[3] = best[0];
-  P.tune_ms[1] = best[1];
-  P.tuned = best[1] < 0.95f * best[0] ? 1 : 3;
+  P.tune_ms[kCands[0]] = best[0];
+  P.tune_ms[kCands[1]] = best[1];
+  P.tuned = best[1] < 0.95f * best[0] ? kCands[1] : kCands[0];
   return P.tuned;
 }
 
@@ -505,7 +579,7 @@ void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, doub
   const bool aligned = ((uintptr_t)b % 16 == 0) && ((uintptr_t)M.x % 16 == 0) && ((uintptr_t)M.out % 16 == 0);
   const bool nd4 = S.uniform_nsf == 4 && aligned;
   int variant = S.mult_variant;
-  if (nd4 && variant == kVariantAuto) variant = tuned_variant(S, P, M, exact);
+  if (variant == kVariantAuto) variant = tuned_variant(S, P, M, exact, nd4);
   cudaEvent_t ev0 = nullptr;
   if (S.prof.on) { ev0 = S.prof.get(); CQ_CUDA(cudaEventRecord(ev0, st)); }
   launch_variant(S, P, M, variant, exact, nd4);

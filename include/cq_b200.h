@@ -115,7 +115,7 @@ int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, doub
 int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* triples, int64_t* flops);
 
 /* Autotuner record of one product: the FP64 kernel variant it chose (-1 before the product's
- * first autotuned call) and the timed milliseconds of each candidate variant (ms[4], 0 = not timed). */
+ * first autotuned call) and the timed milliseconds of each candidate variant (ms[5], 0 = not timed). */
 int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int* variant, float* ms);
 
 /*
@@ -178,7 +178,9 @@ int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out)
  * events and keeps the faster), 0 = one lane per output element, 1 = one thread per output
  * block, 2 = one thread per output block with the first operand's row staged in shared memory,
  * 3 = one thread per output block with the warp staging the operand blocks through shared
- * memory.  All give identical results.
+ * memory; for other block sizes (DZP 13 x 13, mixed sizes) 0 = one warp per output block, one lane
+ * per element, 4 = one warp per output block, a 4 x 2 register tile per lane (the autotuner
+ * candidates are 3/1 for uniform 4 x 4 blocks and 4/0 otherwise).  All give identical results.
  * CQ_OPT_BLOCKING_SYNC: 1 = the host thread sleeps on a blocking-sync event whenever the
  * solver waits for a scalar from the device (many concurrent solvers per host core), 0 = it
  * spins in cudaStreamSynchronize (default, lowest latency for one solver). */

@@ -53,8 +53,10 @@ def _abs_bound(o, mult_type, ra, rb, rc, a, b, c):
     return out
 
 
-def test_type1_dzp_bit_exact(cfg1):
+@pytest.mark.parametrize("variant", [-1, 0, 4])
+def test_type1_dzp_bit_exact(cfg1, variant):
     o, g, bls = cfg1
+    g.set_mult_variant(variant)
     a = inputs.random_blocks(bls[0], 11, inputs.TAG_RANDOM_A)
     b = inputs.random_blocks(bls[1], 11, inputs.TAG_RANDOM_B)
     c_ref = np.zeros(bls[2].length)
@@ -92,8 +94,10 @@ def test_bf16x3_tensor_core_products(cfg1, mult_type):
     assert err.max() > 0          # it really ran in reduced precision
 
 
-def test_type2_dzp_bit_exact(cfg1):
+@pytest.mark.parametrize("variant", [-1, 0, 4])
+def test_type2_dzp_bit_exact(cfg1, variant):
     o, g, bls = cfg1
+    g.set_mult_variant(variant)
     b = inputs.random_blocks(bls[1], 12, inputs.TAG_RANDOM_B)
     cin = inputs.random_blocks(bls[2], 12, inputs.TAG_RANDOM_A)
     out_ref = np.zeros(bls[0].length)
@@ -101,6 +105,30 @@ def test_type2_dzp_bit_exact(cfg1):
     out = np.full(bls[0].length, np.nan)
     g.mat_mult_host(2, 0, 1, 2, out, b, cin, exact=True)
     assert np.array_equal(out, out_ref)
+
+
+@pytest.mark.parametrize("variant", [0, 4])
+@pytest.mark.parametrize("mult_type", [1, 2])
+def test_mixed_block_sizes_bit_exact(variant, mult_type):
+    """Atoms with 4 and 13 orbitals in one system: every block shape (4x4, 4x13, 13x4, 13x13)."""
+    import cq_b200
+    coords, cell = inputs.diamond_si(2, sigma=0.05, seed=21)
+    nsf = np.where(np.arange(len(coords)) % 3 == 0, 13, 4).astype(np.int32)
+    rc = [6.0, 8.0, 14.0]
+    o = OracleSystem(coords, cell, nsf, rc)
+    g = cq_b200.System(coords, cell, nsf, rc)
+    g.set_mult_variant(variant)
+    bls = [bm.oracle_blocklist(o, r, coords, cell) for r in range(3)]
+    b = inputs.random_blocks(bls[1], 31, inputs.TAG_RANDOM_B)
+    if mult_type == 1:
+        a = inputs.random_blocks(bls[0], 31, inputs.TAG_RANDOM_A)
+        ref = np.zeros(bls[2].length); o.mat_mult(1, 0, 1, 2, a, b, ref)
+        got = np.full(bls[2].length, np.nan); g.mat_mult_host(1, 0, 1, 2, a, b, got)
+    else:
+        cin = inputs.random_blocks(bls[2], 32, inputs.TAG_RANDOM_A)
+        ref = np.zeros(bls[0].length); o.mat_mult(2, 0, 1, 2, ref, b, cin)
+        got = np.full(bls[0].length, np.nan); g.mat_mult_host(2, 0, 1, 2, got, b, cin)
+    assert np.array_equal(got, ref)
 
 
 LNV_PRODUCTS = [  # (type, a range, b range, c range) in mat_mult roles, from the product table of mult_module.f90
