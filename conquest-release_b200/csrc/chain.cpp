@@ -101,7 +101,9 @@ void LNVSolver::solve() {
     CQ_CUDA(cudaMemsetAsync(m->p, 0, sizeof(double) * std::max<int64_t>(m->n, 1), S.stream));
   use_mixed = false;
   invert_S();                       // T = S^-1 in FP64 in both forms
-  if (!prm.mixed) {
+  // no product of this system would run in split precision (mult_dispatch keeps blocks of 8 x 8
+  // or less in FP64): the mixed form is the FP64 solve, in one phase
+  if (!prm.mixed || S.max_nsf <= 8) {
     find_min_dm(true);
     return;
   }
