@@ -67,6 +67,7 @@ int cq_lnv_params_default(cq_lnv_params* p) {
   p->mixed_tolerance = 1.0e-5;
   p->fp64_mcw_sweeps = 0;
   p->graphs = 1;
+  p->mixed_mcw = 0;
   return CQ_OK;
 }
 

@@ -123,7 +123,16 @@ void LNVSolver::solve() {
   use_mixed = false;
   stats.converged = 0;
   if (prm.fp64_mcw_sweeps > 0) purify(prm.fp64_mcw_sweeps);
-  find_min_dm(false);
+  // both phases share the pass limit of the FP64 solve (at least one FP64 pass)
+  const int max_outer = prm.max_outer;
+  prm.max_outer = std::max(1, max_outer - stats.outer_iters);
+  try {
+    find_min_dm(false);
+  } catch (...) {
+    prm.max_outer = max_outer;
+    throw;
+  }
+  prm.max_outer = max_outer;
 }
 
 // McWeeny purification sweeps of L (McW_matrix_multiply_nonds, McWeeny.f90:620-740), kept while
@@ -802,8 +811,14 @@ void LNVSolver::find_min_dm(bool resetL) {
     if (++outer > prm.max_outer) break;
     stats.outer_iters++;
     if (resetL || inflex) {
+      // the McWeeny start runs in FP64 unless mixed_mcw: split-precision noise in its stopping
+      // test (energy rise, |dE| < 1e-8) changes the start, and a truncated functional can then
+      // descend into another minimum than the FP64 solve
+      const bool um = use_mixed;
+      if (!prm.mixed_mcw) use_mixed = false;
       init_mcw();
       delta_e = mcw_min(prm.n_L_iterations);
+      use_mixed = um;
       early = true;
       resetL = false;
     }

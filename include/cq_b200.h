@@ -218,6 +218,8 @@ typedef struct {
   int fp64_mcw_sweeps;     /* FP64 McWeeny purification sweeps of L between the two phases (0) */
   int graphs;              /* 1: each LNV_matrix_multiply call is captured once in a CUDA graph and replayed
                               (same results; default 1) */
+  int mixed_mcw;           /* mixed form: 1 = the McWeeny start also runs split-precision products
+                              (default 0: FP64, the same start as the FP64 solve) */
 } cq_lnv_params;
 
 typedef struct {

@@ -23,6 +23,7 @@ def test_generated_S_H_match_host(nsf):
         bl = g.blocklist(r, coords, cell)
         host = inputs.overlap_S(bl) if which == 0 else inputs.hamiltonian_H(bl, seed=7)
         dev = torch.full((g.length(r),), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()      # torch's stream and the library's stream are different
         g.generate_SH(r, which, 7, dev)
         g.synchronize()
         got = dev.cpu().numpy()

@@ -183,21 +183,24 @@ def test_algebra_matches_oracle(cfg2):
     S = inputs.random_blocks(bls["S"], 41, 2)
     LSL = inputs.random_blocks(bls["LSL"], 41, 3)
     tL, tS, tLSL = (torch.tensor(x, device=dev) for x in (L, S, LSL))
+    # torch works on its default stream and the library on its own: synchronise between them
+    sync = torch.cuda.synchronize
     # same range: scal + axpy
     ref = L.copy(); ref = ref * 0.5; ref = ref + (-2.0 * L)
-    t = tL.clone(); g.matrix_sum(idx["L"], t, 0.5, idx["L"], tL, -2.0); g.synchronize()
+    t = tL.clone(); sync(); g.matrix_sum(idx["L"], t, 0.5, idx["L"], tL, -2.0); g.synchronize()
     assert np.array_equal(t.cpu().numpy(), ref)
     # shorter destination (prune) and longer destination (partial update)
     ref = S.copy(); o.matrix_add(0.0, ref, idx["S"], 3.0, LSL, idx["LSL"])
-    t = tS.clone(); g.matrix_sum(idx["S"], t, 0.0, idx["LSL"], tLSL, 3.0); g.synchronize()
+    t = tS.clone(); sync(); g.matrix_sum(idx["S"], t, 0.0, idx["LSL"], tLSL, 3.0); g.synchronize()
     assert np.array_equal(t.cpu().numpy(), ref)
     ref = L.copy(); o.matrix_add(1.0, ref, idx["L"], -0.25, S, idx["S"])
-    t = tL.clone(); g.matrix_sum(idx["L"], t, 1.0, idx["S"], tS, -0.25); g.synchronize()
+    t = tL.clone(); sync(); g.matrix_sum(idx["L"], t, 1.0, idx["S"], tS, -0.25); g.synchronize()
     assert np.array_equal(t.cpu().numpy(), ref)
     # transpose, traces
     for r in ("L", "LS", "LSL"):
         x = inputs.random_blocks(bls[r], 43, 5)
         tx = torch.tensor(x, device=dev); tt = torch.empty_like(tx)
+        sync()
         g.transpose(idx[r], tx, tt); g.synchronize()
         assert np.array_equal(tt.cpu().numpy(), o.transpose(idx[r], x))
     assert abs(g.trace(idx["L"], tL) - o.trace(idx["L"], L)) < 1e-12 * abs(o.trace(idx["L"], L)) + 1e-14

@@ -74,6 +74,7 @@ def test_server_equals_direct_solver():
     ridx = {n: i for i, n in enumerate(rng)}
     S = torch.zeros(g.length(ridx["S"]), dtype=torch.float64, device="cuda")
     H = torch.zeros(g.length(ridx["H"]), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()          # torch's stream and the library's stream are different
     g.generate_SH(ridx["S"], 0, seed, S)
     g.generate_SH(ridx["H"], 1, seed, H)
     g.synchronize()
