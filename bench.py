@@ -592,7 +592,7 @@ def mult_main(args):
                 ms.append(e0.elapsed_time(e1))
             m = float(np.median(ms))
             nbytes = 8.0 * (g.length(ra) + g.length(rb) + g.length(rc))
-            tv, tms = g.product_tuning(t, ra, rb, rc)
+            tv, tms = g.product_tuning(t, ra, rb, rc, mixed=(args.precision == "bf16x3"))
             out.append({"product": name, "triples": triples, "flops": flops, "ms": m, "tuned_variant": tv,
                         "tune_ms": tms,
                         "tflops": flops / (m / 1e3) / 1e12, "gbs_algorithmic": nbytes / (m / 1e3) / 1e9})

@@ -89,7 +89,8 @@ def lib():
         "cq_mat_mult": [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int],
         "cq_mat_mult_host": [c_void_p, c_int, c_int, c_int, c_int, P(c_double), P(c_double), P(c_double), c_int],
         "cq_product_work": [c_void_p, c_int, c_int, c_int, c_int, P(c_int64), P(c_int64)],
-        "cq_product_tuning": [c_void_p, c_int, c_int, c_int, c_int, P(c_int), P(ctypes.c_float)],
+        "cq_product_tuning": [c_void_p, c_int, c_int, c_int, c_int, P(c_int), P(ctypes.c_float), P(c_int),
+                              P(ctypes.c_float)],
         "cq_matrix_sum": [c_void_p, c_int, c_void_p, c_double, c_int, c_void_p, c_double],
         "cq_matrix_transpose": [c_void_p, c_int, c_void_p, c_void_p],
         "cq_matrix_trace": [c_void_p, c_int, c_void_p, P(c_double)],
@@ -227,11 +228,14 @@ class System:
         check(lib().cq_product_work(self._h, mult_type, ra, rb, rc, ctypes.byref(t), ctypes.byref(f)))
         return t.value, f.value
 
-    def product_tuning(self, mult_type, ra, rb, rc):
-        """(variant chosen by the autotuner or -1, {variant: timed ms}) of one product."""
-        v = c_int()
-        ms = (ctypes.c_float * 5)()
-        check(lib().cq_product_tuning(self._h, mult_type, ra, rb, rc, ctypes.byref(v), ms))
+    def product_tuning(self, mult_type, ra, rb, rc, mixed=False):
+        """FP64: (variant chosen by the autotuner or -1, {variant: timed ms}); mixed=True: (output blocks per
+        warp chosen for the split-precision kernel or -1, {group size: timed ms})."""
+        v, g = c_int(), c_int()
+        ms, gms = (ctypes.c_float * 5)(), (ctypes.c_float * 3)()
+        check(lib().cq_product_tuning(self._h, mult_type, ra, rb, rc, ctypes.byref(v), ms, ctypes.byref(g), gms))
+        if mixed:
+            return g.value, {gs: gms[i] for i, gs in enumerate((2, 4, 8)) if gms[i] > 0}
         return v.value, {i: ms[i] for i in range(5) if ms[i] > 0}
 
     def matrix_sum(self, ra, a, alpha, rb, b, beta):

@@ -638,13 +638,6 @@ MixedPlan& get_mixed_plan(System& S, int mult_type, int ra, int rb, int rc) {
     M.ptr = M.own_ptr.p;
     M.pairs = M.own_pairs.p;
   }
-  // groups of up to 8 consecutive output blocks of one row
-  RangeIndex& O = *S.ranges[M.out_range];
-  std::vector<int2> grp;
-  for (int p = 0; p < S.geo.n_prim; ++p)
-    for (int s = O.h_row_ptr[p]; s < O.h_row_ptr[p + 1]; s += 8) grp.push_back(make_int2(s, std::min(8, O.h_row_ptr[p + 1] - s)));
-  M.n_groups = (int)grp.size();
-  M.groups.upload(grp, st);
   CQ_CUDA(cudaStreamSynchronize(st));
   auto res = S.mplans.emplace(key, std::move(mp));
   return *res.first->second;

@@ -7,7 +7,10 @@
 // the block storage of the output range, so the matrices of the chain stay FP64.
 //
 // Work decomposition (output stationary, same pair lists as the FP64 path):
-// one warp owns G consecutive output blocks of one output row i.  Their pair
+// one warp owns G consecutive output blocks of one output row i (G = 2, 4 or 8, chosen per
+// product by the autotuner: larger groups reuse each first-operand fragment more, smaller ones
+// need fewer registers and give more warps; the results do not depend on G, since each output
+// block accumulates its own pairs in its own order).  Their pair
 // lists are sorted by the first operand block (A_ik for type 1, C_ij for type 2,
 // both in row i), so the warp walks the union of those blocks in order, loads each
 // first-operand fragment once and multiplies it into every output block whose list
@@ -22,7 +25,6 @@
 namespace cqb {
 namespace {
 
-constexpr int kG = 8;   // output blocks per warp
 
 __device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo_k, __nv_bfloat16 hi_k) {
   return (uint32_t)__bfloat16_as_ushort(lo_k) | ((uint32_t)__bfloat16_as_ushort(hi_k) << 16);
@@ -103,6 +105,7 @@ struct TCArgs {
   double* __restrict__ out;
 };
 
+template <int kG>   // output blocks per warp
 __global__ void __launch_bounds__(128) k_mult_tc(TCArgs M) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (w >= M.n_groups) return;
@@ -195,22 +198,69 @@ void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a,
   launch_mult_tc(S, MP, fx.hi.p, fx.lo.p, fb.hi.p, fb.lo.p, out);
 }
 
+static void launch_tc_g(System& S, MixedPlan& MP, TCArgs M, int gi) {
+  static const int kGs[3] = {2, 4, 8};
+  if (MP.n_groups[gi] < 0) {
+    // groups of up to G consecutive output blocks of one row
+    RangeIndex& O = *S.ranges[MP.out_range];
+    const int G = kGs[gi];
+    std::vector<int2> grp;
+    for (int p = 0; p < S.geo.n_prim; ++p)
+      for (int s0 = O.h_row_ptr[p]; s0 < O.h_row_ptr[p + 1]; s0 += G)
+        grp.push_back(make_int2(s0, std::min(G, O.h_row_ptr[p + 1] - s0)));
+    MP.n_groups[gi] = (int)grp.size();
+    MP.groups[gi].upload(grp, S.stream);
+  }
+  M.groups = MP.groups[gi].p;
+  M.n_groups = MP.n_groups[gi];
+  if (M.n_groups == 0) return;
+  const int grid = (M.n_groups * 32 + 127) / 128;
+  if (gi == 0) k_mult_tc<2><<<grid, 128, 0, S.stream>>>(M);
+  else if (gi == 1) k_mult_tc<4><<<grid, 128, 0, S.stream>>>(M);
+  else k_mult_tc<8><<<grid, 128, 0, S.stream>>>(M);
+  S.launches++;
+  CQ_CUDA(cudaGetLastError());
+}
+
 void launch_mult_tc(System& S, MixedPlan& MP, const uint4* xa_hi, const uint4* xa_lo, const uint4* bb_hi,
                     const uint4* bb_lo, double* out) {
   RangeIndex& O = *S.ranges[MP.out_range];
   TCArgs M;
-  M.groups = MP.groups.p;
-  M.n_groups = MP.n_groups;
   M.ptr = MP.ptr;
   M.pairs = MP.pairs;
   M.xa_hi = xa_hi; M.xa_lo = xa_lo; M.bb_hi = bb_hi; M.bb_lo = bb_lo;
   M.o_row = O.nb_row.p; M.o_cover = O.nb_cover.p; M.o_elem = O.nb_elem.p;
   M.prim_nsf = S.dg.prim_nsf.p; M.cover_nsf = S.dg.cover_nsf.p;
   M.out = out;
-  if (MP.n_groups == 0) return;
-  k_mult_tc<<<(MP.n_groups * 32 + 127) / 128, 128, 0, S.stream>>>(M);
-  S.launches++;
-  CQ_CUDA(cudaGetLastError());
+  if (O.nnz == 0) return;
+  if (MP.tuned_g < 0) {
+    // autotuner: each group size once warm, then three interleaved timed rounds; the fastest
+    // round counts, G = 8 is kept unless another size is 5 % faster.  Every launch overwrites
+    // the whole output with the same values.
+    cudaEvent_t e0, e1;
+    CQ_CUDA(cudaEventCreate(&e0));
+    CQ_CUDA(cudaEventCreate(&e1));
+    float best[3] = {1e30f, 1e30f, 1e30f};
+    for (int gi = 0; gi < 3; ++gi) launch_tc_g(S, MP, M, gi);
+    for (int round = 0; round < 3; ++round)
+      for (int gi = 0; gi < 3; ++gi) {
+        CQ_CUDA(cudaEventRecord(e0, S.stream));
+        launch_tc_g(S, MP, M, gi);
+        CQ_CUDA(cudaEventRecord(e1, S.stream));
+        CQ_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best[gi] = std::min(best[gi], ms);
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int pick = 2;
+    for (int gi = 0; gi < 2; ++gi)
+      if (best[gi] < 0.95f * best[pick]) pick = gi;
+    for (int gi = 0; gi < 3; ++gi) MP.tune_ms[gi] = best[gi];
+    MP.tuned_g = pick;
+  }
+  launch_tc_g(S, MP, M, MP.tuned_g);
 }
 
 }  // namespace cqb

@@ -115,8 +115,11 @@ int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, doub
 int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* triples, int64_t* flops);
 
 /* Autotuner record of one product: the FP64 kernel variant it chose (-1 before the product's
- * first autotuned call) and the timed milliseconds of each candidate variant (ms[5], 0 = not timed). */
-int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int* variant, float* ms);
+ * first autotuned call) and the timed milliseconds of each candidate variant (ms[5], 0 = not
+ * timed); for its split-precision form the output blocks per warp it chose (2, 4 or 8; -1 = not
+ * tuned yet) and the timed milliseconds of those three group sizes (group_ms[3]). */
+int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int* variant, float* ms, int* group,
+                      float* group_ms);
 
 /*
  * Drop-in kernel pair (plugin surface of multiply_kernel_<MULT_KERN>.f90):
