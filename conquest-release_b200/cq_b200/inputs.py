@@ -10,8 +10,12 @@ bit-identical inputs once both have laid out the same neighbour lists.
 
 Generators (per image-resolved atom pair at distance r, blocks nd_i x nd_j):
   * random blocks: uniform[-1, 1] * exp(-r / 3)                 (mat_mult KAT)
-  * S: onsite 1.0 * I, offsite 0.3 * exp(-r / 2) every entry     (overlap)
-  * H: onsite symmetrised uniform[-0.5, 0], offsite -0.2 * exp(-r / 2)
+  * S: onsite 1.0 * I, offsite 0.3 * exp(-r / 2) * w every entry (overlap)
+  * H: onsite diagonal uniform[-0.5, 0], offsite -0.2 * exp(-r / 2) * w
+with the block weight w = min(1, 4 / sqrt(nd_i nd_j)).  For 4 x 4 (SZ) blocks w = 1 and the entries
+are the stated ones; for larger blocks an offsite block whose every entry equals 0.3 exp(-r/2) has
+a row sum nd_j times larger, and with 13 x 13 (DZP) blocks the overlap of diamond Si is no longer
+diagonally dominant (nor positive definite), so the weight keeps the row sums of the SZ case.
 """
 from __future__ import annotations
 
@@ -126,10 +130,15 @@ def _onsite_mask(bl, sel):
     return (bl.ig_i[sel] == bl.ig_j[sel]) & np.all(bl.shift[sel] == 0, axis=1)
 
 
+def block_weight(ndi, ndj):
+    """Offsite weight of an nd_i x nd_j block: 1 for SZ blocks, 4 / sqrt(nd_i nd_j) for larger ones."""
+    return min(1.0, 4.0 / np.sqrt(float(ndi) * float(ndj)))
+
+
 def overlap_S(bl):
-    """S: 1.0 * I on the onsite block, 0.3 * exp(-r/2) on every entry of an offsite block."""
+    """S: 1.0 * I on the onsite block, 0.3 * exp(-r/2) * w on every entry of an offsite block."""
     def fn(sel, ndi, ndj, e):
-        v = np.repeat((0.3 * np.exp(-bl.radius[sel] / 2.0))[:, None], e.size, axis=1)
+        v = np.repeat((0.3 * block_weight(ndi, ndj) * np.exp(-bl.radius[sel] / 2.0))[:, None], e.size, axis=1)
         on = _onsite_mask(bl, sel)
         if on.any():
             eye = (e % ndi == e // ndi).astype(np.float64)
@@ -139,7 +148,7 @@ def overlap_S(bl):
 
 
 def hamiltonian_H(bl, seed):
-    """H: onsite block diagonal with orbital energies uniform[-0.5, 0], offsite -0.2 * exp(-r/2) per entry.
+    """H: onsite block diagonal with orbital energies uniform[-0.5, 0], offsite -0.2 * exp(-r/2) * w per entry.
 
     The onsite block is kept diagonal (hence symmetric): with uniform off-diagonal onsite entries as
     well, the Gershgorin-type estimate of the McWeeny initialisation (onsite |H| added to both
@@ -147,7 +156,7 @@ def hamiltonian_H(bl, seed):
     valid starting point.
     """
     def fn(sel, ndi, ndj, e):
-        v = np.repeat((-0.2 * np.exp(-bl.radius[sel] / 2.0))[:, None], e.size, axis=1)
+        v = np.repeat((-0.2 * block_weight(ndi, ndj) * np.exp(-bl.radius[sel] / 2.0))[:, None], e.size, axis=1)
         on = _onsite_mask(bl, sel)
         if on.any():
             r_, c_ = e % ndi, e // ndi

@@ -1,8 +1,10 @@
 // Device-side synthetic S and H (the generators of cq_b200/inputs.py, evaluated on the GPU so a
 // request never round-trips its matrices through the host):
-//   S: onsite block 1.0 * I, offsite 0.3 exp(-r/2) on every entry
+//   S: onsite block 1.0 * I, offsite 0.3 exp(-r/2) w on every entry
 //   H: onsite block diagonal with -0.5 u (u uniform [0,1) from the counter hash of
-//      (seed, tag 21, atom, atom, 0, 0, 0, orbital)), offsite -0.2 exp(-r/2) on every entry
+//      (seed, tag 21, atom, atom, 0, 0, 0, orbital)), offsite -0.2 exp(-r/2) w on every entry
+// with the block weight w = min(1, 4 / sqrt(nd_i nd_j)) (1 for SZ blocks; it keeps the overlap of
+// larger blocks diagonally dominant).
 // The hash is integer arithmetic identical to inputs.hash_uniform; exp() may differ from the
 // host's libm in the last bit.
 #include "cq_internal.hpp"
@@ -42,7 +44,8 @@ __global__ void k_gen_SH(int nnz, int which, uint64_t seed, const int* __restric
   const int gi = prim_global[p], gj = cover_global[c];
   const int* sh = cover_shift + 3 * cover_part[c];
   const bool onsite = gi == gj && sh[0] == 0 && sh[1] == 0 && sh[2] == 0;
-  const double off = (which == 0 ? 0.3 : -0.2) * exp(-nb_radius[e] / 2.0);
+  const double w = fmin(1.0, 4.0 / sqrt((double)ndi * (double)ndj));
+  const double off = (which == 0 ? 0.3 : -0.2) * w * exp(-nb_radius[e] / 2.0);
   double* O = out + nb_elem[e];
   for (int t = lane; t < ndi * ndj; t += 32) {
     const int r = t % ndi, col = t / ndi;
