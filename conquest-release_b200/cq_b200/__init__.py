@@ -232,10 +232,10 @@ class System:
         """FP64: (variant chosen by the autotuner or -1, {variant: timed ms}); mixed=True: (output blocks per
         warp chosen for the split-precision kernel or -1, {group size: timed ms})."""
         v, g = c_int(), c_int()
-        ms, gms = (ctypes.c_float * 5)(), (ctypes.c_float * 3)()
+        ms, gms = (ctypes.c_float * 5)(), (ctypes.c_float * 4)()
         check(lib().cq_product_tuning(self._h, mult_type, ra, rb, rc, ctypes.byref(v), ms, ctypes.byref(g), gms))
         if mixed:
-            return g.value, {gs: gms[i] for i, gs in enumerate((2, 4, 8)) if gms[i] > 0}
+            return g.value, {gs: gms[i] for i, gs in enumerate((1, 2, 4, 8)) if gms[i] > 0}
         return v.value, {i: ms[i] for i in range(5) if ms[i] > 0}
 
     def matrix_sum(self, ra, a, alpha, rb, b, beta):

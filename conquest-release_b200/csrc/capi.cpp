@@ -244,9 +244,9 @@ int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int
     if (ms) for (int v = 0; v < 5; ++v) ms[v] = P.tune_ms[v];
     auto it = sys->S.mplans.find(std::make_tuple(mult_type, ra, rb, rc));
     const MixedPlan* M = it == sys->S.mplans.end() ? nullptr : it->second.get();
-    static const int kGs[3] = {2, 4, 8};
+    static const int kGs[4] = {1, 2, 4, 8};
     if (group) *group = (M && M->tuned_g >= 0) ? kGs[M->tuned_g] : -1;
-    if (group_ms) for (int g = 0; g < 3; ++g) group_ms[g] = M ? M->tune_ms[g] : 0.f;
+    if (group_ms) for (int g = 0; g < 4; ++g) group_ms[g] = M ? M->tune_ms[g] : 0.f;
   });
 }
 

@@ -214,15 +214,15 @@ struct ProductPlan {
 // and groups of consecutive output blocks of one row (one warp each).
 struct MixedPlan {
   int mult_type = 1, ra = -1, rb = -1, rc = -1, out_range = -1;
-  int n_groups[3] = {-1, -1, -1};   // groups of 2, 4 and 8 output blocks (-1: not built yet)
-  int tuned_g = -1;                 // group size chosen by the autotuner (index into 2, 4, 8)
-  float tune_ms[3] = {0, 0, 0};
+  int n_groups[4] = {-1, -1, -1, -1};   // groups of 1, 2, 4 and 8 output blocks (-1: not built yet)
+  int tuned_g = -1;                 // group size chosen by the autotuner (index into 1, 2, 4, 8)
+  float tune_ms[4] = {0, 0, 0, 0};
   int64_t n_pairs = 0, flops = 0;
   DevBuf<int64_t> own_ptr;        // type 2 only (type 1 uses the FP64 plan's lists, already sorted)
   DevBuf<int2> own_pairs;
   const int64_t* ptr = nullptr;
   const int2* pairs = nullptr;
-  DevBuf<int2> groups[3];
+  DevBuf<int2> groups[4];
 };
 
 struct FragBuf { DevBuf<uint4> hi, lo; };

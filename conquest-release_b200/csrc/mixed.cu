@@ -7,7 +7,7 @@
 // the block storage of the output range, so the matrices of the chain stay FP64.
 //
 // Work decomposition (output stationary, same pair lists as the FP64 path):
-// one warp owns G consecutive output blocks of one output row i (G = 2, 4 or 8, chosen per
+// one warp owns G consecutive output blocks of one output row i (G = 1, 2, 4 or 8, chosen per
 // product by the autotuner: larger groups reuse each first-operand fragment more, smaller ones
 // need fewer registers and give more warps; the results do not depend on G, since each output
 // block accumulates its own pairs in its own order).  Their pair
@@ -199,7 +199,7 @@ void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a,
 }
 
 static void launch_tc_g(System& S, MixedPlan& MP, TCArgs M, int gi) {
-  static const int kGs[3] = {2, 4, 8};
+  static const int kGs[4] = {1, 2, 4, 8};
   if (MP.n_groups[gi] < 0) {
     // groups of up to G consecutive output blocks of one row
     RangeIndex& O = *S.ranges[MP.out_range];
@@ -215,8 +215,9 @@ static void launch_tc_g(System& S, MixedPlan& MP, TCArgs M, int gi) {
   M.n_groups = MP.n_groups[gi];
   if (M.n_groups == 0) return;
   const int grid = (M.n_groups * 32 + 127) / 128;
-  if (gi == 0) k_mult_tc<2><<<grid, 128, 0, S.stream>>>(M);
-  else if (gi == 1) k_mult_tc<4><<<grid, 128, 0, S.stream>>>(M);
+  if (gi == 0) k_mult_tc<1><<<grid, 128, 0, S.stream>>>(M);
+  else if (gi == 1) k_mult_tc<2><<<grid, 128, 0, S.stream>>>(M);
+  else if (gi == 2) k_mult_tc<4><<<grid, 128, 0, S.stream>>>(M);
   else k_mult_tc<8><<<grid, 128, 0, S.stream>>>(M);
   S.launches++;
   CQ_CUDA(cudaGetLastError());
@@ -235,15 +236,15 @@ void launch_mult_tc(System& S, MixedPlan& MP, const uint4* xa_hi, const uint4* x
   if (O.nnz == 0) return;
   if (MP.tuned_g < 0) {
     // autotuner: each group size once warm, then three interleaved timed rounds; the fastest
-    // round counts, G = 8 is kept unless another size is 5 % faster.  Every launch overwrites
+    // round counts, and a smaller group replaces a larger one only when it is 5 % faster.  Every launch overwrites
     // the whole output with the same values.
     cudaEvent_t e0, e1;
     CQ_CUDA(cudaEventCreate(&e0));
     CQ_CUDA(cudaEventCreate(&e1));
-    float best[3] = {1e30f, 1e30f, 1e30f};
-    for (int gi = 0; gi < 3; ++gi) launch_tc_g(S, MP, M, gi);
+    float best[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+    for (int gi = 0; gi < 4; ++gi) launch_tc_g(S, MP, M, gi);
     for (int round = 0; round < 3; ++round)
-      for (int gi = 0; gi < 3; ++gi) {
+      for (int gi = 0; gi < 4; ++gi) {
         CQ_CUDA(cudaEventRecord(e0, S.stream));
         launch_tc_g(S, MP, M, gi);
         CQ_CUDA(cudaEventRecord(e1, S.stream));
@@ -254,10 +255,10 @@ void launch_mult_tc(System& S, MixedPlan& MP, const uint4* xa_hi, const uint4* x
       }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    int pick = 2;
-    for (int gi = 0; gi < 2; ++gi)
+    int pick = 3;
+    for (int gi = 0; gi < 3; ++gi)
       if (best[gi] < 0.95f * best[pick]) pick = gi;
-    for (int gi = 0; gi < 3; ++gi) MP.tune_ms[gi] = best[gi];
+    for (int gi = 0; gi < 4; ++gi) MP.tune_ms[gi] = best[gi];
     MP.tuned_g = pick;
   }
   launch_tc_g(S, MP, M, MP.tuned_g);

@@ -116,8 +116,8 @@ int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64
 
 /* Autotuner record of one product: the FP64 kernel variant it chose (-1 before the product's
  * first autotuned call) and the timed milliseconds of each candidate variant (ms[5], 0 = not
- * timed); for its split-precision form the output blocks per warp it chose (2, 4 or 8; -1 = not
- * tuned yet) and the timed milliseconds of those three group sizes (group_ms[3]). */
+ * timed); for its split-precision form the output blocks per warp it chose (1, 2, 4 or 8; -1 =
+ * not tuned yet) and the timed milliseconds of those four group sizes (group_ms[4]). */
 int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int* variant, float* ms, int* group,
                       float* group_ms);
 
