@@ -32,7 +32,7 @@ class LNVParams(ctypes.Structure):
                 ("maxpulaystep", c_double), ("lintol", c_double), ("global_tolerance", c_int), ("vary_mu", c_int),
                 ("invs_max_steps", c_int), ("invs_delta_tol", c_double), ("invs_tol", c_double), ("exact", c_int),
                 ("max_outer", c_int), ("mixed", c_int), ("mixed_tolerance", c_double), ("fp64_mcw_sweeps", c_int),
-                ("graphs", c_int), ("mixed_mcw", c_int)]
+                ("graphs", c_int), ("mixed_mcw", c_int), ("fp64_continue", c_int)]
 
 
 class LNVResult(ctypes.Structure):

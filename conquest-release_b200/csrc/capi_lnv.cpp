@@ -68,6 +68,7 @@ int cq_lnv_params_default(cq_lnv_params* p) {
   p->fp64_mcw_sweeps = 0;
   p->graphs = 1;
   p->mixed_mcw = 0;
+  p->fp64_continue = 1;
   return CQ_OK;
 }
 

@@ -121,8 +121,17 @@ void LNVSolver::solve() {
   }
   prm.tolerance = tol;
   use_mixed = false;
-  stats.converged = 0;
   if (prm.fp64_mcw_sweeps > 0) purify(prm.fp64_mcw_sweeps);
+  if (!prm.fp64_continue) {
+    // finish without further minimisation: the purified L, with K, the band energy and the
+    // electron count evaluated in FP64 (errors in L enter the energy at second order)
+    double el = 0, en = 0;
+    lnv(true, false, true, true, nullptr, &phi, &el, &en);
+    stats.energy = 2.0 * en;
+    stats.electrons = 2.0 * el;
+    return;
+  }
+  stats.converged = 0;
   // both phases share the pass limit of the FP64 solve (at least one FP64 pass)
   const int max_outer = prm.max_outer;
   prm.max_outer = std::max(1, max_outer - stats.outer_iters);

@@ -223,6 +223,9 @@ typedef struct {
                               (same results; default 1) */
   int mixed_mcw;           /* mixed form: 1 = the McWeeny start also runs split-precision products
                               (default 0: FP64, the same start as the FP64 solve) */
+  int fp64_continue;       /* mixed form: 1 = FindMinDM continues in FP64 to `tolerance` (default);
+                              0 = after the split-precision phase only the FP64 purification sweeps
+                              (fp64_mcw_sweeps) and an FP64 evaluation of K, energy and electrons */
 } cq_lnv_params;
 
 typedef struct {
