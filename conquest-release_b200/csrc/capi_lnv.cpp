@@ -64,7 +64,7 @@ int cq_lnv_params_default(cq_lnv_params* p) {
   p->exact = 1;
   p->max_outer = 40;
   p->mixed = 0;
-  p->mixed_tolerance = 1.0e-5;
+  p->mixed_tolerance = 1.0e-6;
   p->fp64_mcw_sweeps = 0;
   p->graphs = 1;
   p->mixed_mcw = 0;

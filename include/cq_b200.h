@@ -217,7 +217,7 @@ typedef struct {
   int mixed;               /* 1: cq_lnv_solve runs FindMinDM (McWeeny start included) with CQ_PREC_BF16X3
                               products to `mixed_tolerance`, then continues from that L with FP64 products
                               to `tolerance`; Hotelling, traces, line search and Pulay stay FP64 */
-  double mixed_tolerance;  /* residual at which the split-precision phase hands over to FP64 */
+  double mixed_tolerance;  /* residual at which the split-precision phase hands over to FP64 (1e-6) */
   int fp64_mcw_sweeps;     /* FP64 McWeeny purification sweeps of L between the two phases (0) */
   int graphs;              /* 1: each LNV_matrix_multiply call is captured once in a CUDA graph and replayed
                               (same results; default 1) */
