@@ -189,6 +189,14 @@ __global__ void __launch_bounds__(kT) k_acc_final(const uint64_t* __restrict__ p
   block_acc_reduce(a, out);
   if (threadIdx.x == 0) out[3] = (uint64_t)(uint32_t)flags[0] | ((uint64_t)(uint32_t)flags[1] << 32);
 }
+// store_matrix_value(..., j, j, one) on every onsite block: the diagonal of each atom's self block
+__global__ void k_set_onsite_diag(int n_prim, const int64_t* __restrict__ onsite, const int* __restrict__ prim_nsf,
+                                  double value, double* __restrict__ a) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_prim) return;
+  const int nd = prim_nsf[p];
+  for (int j = 0; j < nd; ++j) a[onsite[p] + j * nd + j] = value;
+}
 // onsite diagonal elements gathered for the exact trace
 __global__ void k_gather_diag(int n_prim, const int64_t* __restrict__ onsite, const int* __restrict__ prim_nsf,
                               const int* __restrict__ diag_off, const double* __restrict__ a, double* __restrict__ out) {
@@ -390,6 +398,14 @@ double dev_trace(System& S, int r, const double* a) {
   S.launches++;
   CQ_CUDA(cudaGetLastError());
   return exact_sum(S, S.diag_buf.p, nullptr, (int64_t)S.diag_buf.n);
+}
+void dev_set_onsite_diag(System& S, int r, double* a, double value) {
+  RangeIndex& R = *S.ranges[r];
+  const int N = S.geo.n_prim;
+  if (N == 0) return;
+  k_set_onsite_diag<<<(N + kT - 1) / kT, kT, 0, S.stream>>>(N, R.onsite.p, S.dg.prim_nsf.p, value, a);
+  S.launches++;
+  CQ_CUDA(cudaGetLastError());
 }
 void dev_h_limits(System& S, int r, const double* h, double* hmin, double* hmax) {
   RangeIndex& R = *S.ranges[r];

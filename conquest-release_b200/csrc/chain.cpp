@@ -201,16 +201,7 @@ void LNVSolver::copy(DMat& dst, const DMat& src) { dev_copy(S, dst.p, src.p, src
 
 void LNVSolver::set_identity_onsite(DMat& A) {
   // store_matrix_value(..., j, j, one) on every onsite block
-  std::vector<int64_t> ons = S.ranges[R[A.rng]]->onsite.download(S.stream);
-  std::vector<double> h(A.n, 0.0);
-  CQ_CUDA(cudaMemcpyAsync(h.data(), A.p, sizeof(double) * A.n, cudaMemcpyDeviceToHost, S.stream));
-  host_wait(S);
-  for (int p = 0; p < S.geo.n_prim; ++p) {
-    int nd = S.geo.nsf[S.geo.prim_global[p]];
-    for (int j = 0; j < nd; ++j) h[ons[p] + j * nd + j] = 1.0;
-  }
-  CQ_CUDA(cudaMemcpyAsync(A.p, h.data(), sizeof(double) * A.n, cudaMemcpyHostToDevice, S.stream));
-  host_wait(S);
+  dev_set_onsite_diag(S, R[A.rng], A.p, 1.0);
 }
 
 // ---------------------------------------------------------------------------

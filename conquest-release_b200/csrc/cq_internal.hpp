@@ -326,5 +326,6 @@ void dev_dots_enqueue(System& S, int count, const double* const* x, const double
 void dev_dots_fetch(System& S, int count, double* out);
 double dev_trace(System& S, int r, const double* a);
 void dev_h_limits(System& S, int r, const double* h, double* hmin, double* hmax);
+void dev_set_onsite_diag(System& S, int r, double* a, double value);   // diagonal of every self block
 
 }  // namespace cqb
