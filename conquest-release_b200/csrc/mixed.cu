@@ -165,6 +165,57 @@ __global__ void __launch_bounds__(128) k_mult_tc(TCArgs M) {
   }
 }
 
+// One output block per warp with the next term's four fragments loaded while the current term's
+// six MMAs run (the group-of-one case of k_mult_tc, same terms in the same order, so the same
+// result): the fragment loads of consecutive terms overlap instead of stalling each term.
+__global__ void __launch_bounds__(128) k_mult_tc1(TCArgs M) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= M.n_groups) return;
+  const int q = M.groups[w].x;
+  int64_t p = M.ptr[q];
+  const int64_t pe = M.ptr[q + 1];
+  float acc[2][4];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) acc[h][r] = 0.f;
+  uint4 ah = {0, 0, 0, 0}, al = ah, bh = ah, bl = ah;
+  if (p < pe) {
+    const int2 pr = M.pairs[p];
+    ah = __ldg(M.xa_hi + (int64_t)pr.x * 32 + lane);
+    al = __ldg(M.xa_lo + (int64_t)pr.x * 32 + lane);
+    bh = __ldg(M.bb_hi + (int64_t)pr.y * 32 + lane);
+    bl = __ldg(M.bb_lo + (int64_t)pr.y * 32 + lane);
+  }
+  for (; p < pe; ++p) {
+    uint4 nah = ah, nal = al, nbh = bh, nbl = bl;
+    if (p + 1 < pe) {
+      const int2 pn = M.pairs[p + 1];
+      nah = __ldg(M.xa_hi + (int64_t)pn.x * 32 + lane);
+      nal = __ldg(M.xa_lo + (int64_t)pn.x * 32 + lane);
+      nbh = __ldg(M.bb_hi + (int64_t)pn.y * 32 + lane);
+      nbl = __ldg(M.bb_lo + (int64_t)pn.y * 32 + lane);
+    }
+    mma_bf16(acc[0], al, bh.x, bh.y);
+    mma_bf16(acc[0], ah, bl.x, bl.y);
+    mma_bf16(acc[0], ah, bh.x, bh.y);
+    mma_bf16(acc[1], al, bh.z, bh.w);
+    mma_bf16(acc[1], ah, bl.z, bl.w);
+    mma_bf16(acc[1], ah, bh.z, bh.w);
+    ah = nah; al = nal; bh = nbh; bl = nbl;
+  }
+  const int g = lane >> 2, t = lane & 3;
+  const int ndr = M.prim_nsf[M.o_row[q]], ndc = M.cover_nsf[M.o_cover[q]];
+  double* O = M.out + M.o_elem[q];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      int row = g + ((r & 2) ? 8 : 0), col = 8 * h + 2 * t + (r & 1);
+      if (row < ndr && col < ndc) O[row + ndr * col] = (double)acc[h][r];
+    }
+}
+
 }  // namespace
 
 // A-role (first operand) or B-role fragments of a whole range, hi and lo parts (1 KB per block)
@@ -215,7 +266,7 @@ static void launch_tc_g(System& S, MixedPlan& MP, TCArgs M, int gi) {
   M.n_groups = MP.n_groups[gi];
   if (M.n_groups == 0) return;
   const int grid = (M.n_groups * 32 + 127) / 128;
-  if (gi == 0) k_mult_tc<1><<<grid, 128, 0, S.stream>>>(M);
+  if (gi == 0) k_mult_tc1<<<grid, 128, 0, S.stream>>>(M);
   else if (gi == 1) k_mult_tc<2><<<grid, 128, 0, S.stream>>>(M);
   else if (gi == 2) k_mult_tc<4><<<grid, 128, 0, S.stream>>>(M);
   else k_mult_tc<8><<<grid, 128, 0, S.stream>>>(M);

@@ -282,9 +282,11 @@ __global__ void __launch_bounds__(128, 5) k_mult_nd4_warp(MultArgs M, const int*
   const double2* Xg = reinterpret_cast<const double2*>(M.x);
   const double2* Bg = reinterpret_cast<const double2*>(M.b);
   const int chunk = lane & 7;
+  int2 pr_next = t < tend ? M.pairs[t] : make_int2(-1, -1);   // pair of the next step, loaded a step ahead
   while (__any_sync(kFull, t < tend)) {
     const bool act = t < tend;
-    const int2 pr = act ? M.pairs[t] : make_int2(-1, -1);
+    const int2 pr = pr_next;
+    pr_next = t + 1 < tend ? M.pairs[t + 1] : make_int2(-1, -1);
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int src = 4 * j + (lane >> 3);
