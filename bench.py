@@ -188,6 +188,22 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(x, dist=None, device=None):
+    """The largest value of x over all ranks (replicas are timed by their slowest rank); x itself
+    without a process group."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(units_per_rank, world_size, seconds):
+    """Whole-job throughput of independent replicas: every rank processed units_per_rank in at most `seconds`."""
+    return world_size * units_per_rank / seconds
+
+
 def emit(line):
     print(json.dumps(line), flush=True)
 
@@ -337,12 +353,8 @@ def main():
     prof_step_ms = p0.elapsed_time(p1)
     prof = system.profile_read()
     system.profile(False)
-    t_max = total_ms
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = ws * args.steps / (t_max / 1e3)
+    t_max = max_over_ranks(total_ms, dist, dev)
+    value = replica_rate(args.steps, ws, t_max / 1e3)
     # ---- end to end through the host-memory C ABI call (pinned host S, H in; L, K out)
     pinS = torch.from_numpy(prob["S"]).pin_memory()
     pinH = torch.from_numpy(prob["H"]).pin_memory()
@@ -357,12 +369,8 @@ def main():
     for _ in range(e2e_steps):
         solve_host_pinned(solver, pinS, pinH, pinL, pinK)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = ws * e2e_steps / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    e2e_value = replica_rate(e2e_steps, ws, e2e_s)
     if rank == 0:
         peak, peak_kind = load_peaks()
         achieved = prof["bytes"] / (prof["ms"] / 1e3) / 1e9 if prof["ms"] > 0 else 0.0
