@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <functional>
@@ -175,9 +176,10 @@ class Server {
 
   void worker(int slot) {
     cudaStream_t st = nullptr;
+    cudaError_t setup = cudaSuccess;
     if (!cfg_.dry_run) {
-      cudaSetDevice(device_);
-      cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+      setup = cudaSetDevice(device_);
+      if (setup == cudaSuccess) setup = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     }
     for (;;) {
       std::unique_ptr<Request> q;
@@ -204,6 +206,10 @@ class Server {
       if (cfg_.dry_run) {
         std::this_thread::sleep_for(std::chrono::duration<double>(cfg_.dry_run_seconds));
         res.status = CQ_OK;
+      } else if (setup != cudaSuccess) {
+        // this slot has no device stream: its requests fail with the CUDA error
+        res.status = CQ_ERR_CUDA;
+        std::snprintf(res.message, sizeof(res.message), "slot set-up failed: %s", cudaGetErrorString(setup));
       } else {
         solve(*q, st, res);
       }

@@ -158,7 +158,10 @@ int cq_matrix_product_trace(cq_system* sys, int r, const double* a_dev, const do
 /* Synchronise the system's stream. */
 int cq_synchronize(cq_system* sys);
 
-/* Enqueue all further work of the system on `stream` (a cudaStream_t); NULL restores its own stream. */
+/* Enqueue all further work of the system on `stream` (a cudaStream_t); NULL restores its own stream.
+ * The call synchronises the previous stream first.  A stream given here must stay valid until the
+ * system (and every solver on it) is destroyed: buffers allocated while it was current are released
+ * on it. */
 int cq_system_set_stream(cq_system* sys, void* stream);
 
 /* CUDA-event timing of every block-product launch (timer_module's tmr_std_matmult, per launch). */
