@@ -527,23 +527,28 @@ static void launch_variant(System& S, ProductPlan& P, const MultArgs& M, int var
 
 // Autotuner: on the first call of a product, time the candidate kernels (one warm launch each,
 // then three rounds in which every candidate runs once between CUDA events on the system's
-// stream; a candidate's time is its fastest round) and keep the fastest for the plan, the
-// warp-staged kernel unless another one is at least 5 % faster.  The candidates give identical
+// stream; a candidate's time is its fastest round) and keep the fastest for the plan; a later
+// candidate replaces the preferred one only when it is at least 5 % faster.  The candidates give identical
 // bits and each fully overwrites the output, so tuning changes speed only; the last timed launch
 // leaves the correct result.
 static int tuned_variant(System& S, ProductPlan& P, const MultArgs& M, int exact, bool nd4) {
   if (P.tuned >= 0) return P.tuned;
-  // candidates: the preferred kernel first, the alternative second
-  const int kCands[2] = {nd4 ? 3 : 4, nd4 ? 1 : 0};
+  // candidates, the preferred kernel first: uniform 4x4 blocks: warp-staged, thread per block,
+  // 16 lanes per block (the most parallel, for products with few output blocks); other sizes:
+  // register-tiled, generic
+  int cands[3];
+  int nc = 0;
+  if (nd4) { cands[0] = 3; cands[1] = 1; cands[2] = 0; nc = 3; }
+  else { cands[0] = 4; cands[1] = 0; nc = 2; }
   cudaEvent_t e0, e1;
   CQ_CUDA(cudaEventCreate(&e0));
   CQ_CUDA(cudaEventCreate(&e1));
-  float best[2] = {1e30f, 1e30f};
-  for (int c = 0; c < 2; ++c) launch_variant(S, P, M, kCands[c], exact, nd4);
+  float best[3] = {1e30f, 1e30f, 1e30f};
+  for (int c = 0; c < nc; ++c) launch_variant(S, P, M, cands[c], exact, nd4);
   for (int round = 0; round < 3; ++round)
-    for (int c = 0; c < 2; ++c) {
+    for (int c = 0; c < nc; ++c) {
       CQ_CUDA(cudaEventRecord(e0, S.stream));
-      launch_variant(S, P, M, kCands[c], exact, nd4);
+      launch_variant(S, P, M, cands[c], exact, nd4);
       CQ_CUDA(cudaEventRecord(e1, S.stream));
       CQ_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
@@ -552,9 +557,11 @@ static int tuned_variant(System& S, ProductPlan& P, const MultArgs& M, int exact
     }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  P.tune_ms[kCands[0]] = best[0];
-  P.tune_ms[kCands[1]] = best[1];
-  P.tuned = best[1] < 0.95f * best[0] ? kCands[1] : kCands[0];
+  int pick = 0;
+  for (int c = 1; c < nc; ++c)
+    if (best[c] < 0.95f * best[pick]) pick = c;
+  for (int c = 0; c < nc; ++c) P.tune_ms[cands[c]] = best[c];
+  P.tuned = cands[pick];
   return P.tuned;
 }
 

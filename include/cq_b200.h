@@ -180,13 +180,13 @@ int cq_launch_count(cq_system* sys, int64_t* count);
 int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out);
 
 /* Tuning options.  CQ_OPT_MULT_VARIANT: FP64 4x4 product kernel, -1 = chosen per product by the
- * autotuner (default: the first call of each product times the candidates 1 and 3 with CUDA
- * events and keeps the faster), 0 = one lane per output element, 1 = one thread per output
+ * autotuner (default: the first call of each product times the candidate kernels with CUDA
+ * events and keeps the fastest), 0 = one lane per output element, 1 = one thread per output
  * block, 2 = one thread per output block with the first operand's row staged in shared memory,
  * 3 = one thread per output block with the warp staging the operand blocks through shared
  * memory; for other block sizes (DZP 13 x 13, mixed sizes) 0 = one warp per output block, one lane
  * per element, 4 = one warp per output block, a 4 x 2 register tile per lane (the autotuner
- * candidates are 3/1 for uniform 4 x 4 blocks and 4/0 otherwise).  All give identical results.
+ * candidates are 3/1/0 for uniform 4 x 4 blocks and 4/0 otherwise).  All give identical results.
  * CQ_OPT_BLOCKING_SYNC: 1 = the host thread sleeps on a blocking-sync event whenever the
  * solver waits for a scalar from the device (many concurrent solvers per host core), 0 = it
  * spins in cudaStreamSynchronize (default, lowest latency for one solver). */
