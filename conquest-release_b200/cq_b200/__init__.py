@@ -120,6 +120,7 @@ def lib():
         "cq_lnv_put": [c_void_p, ctypes.c_char_p, c_void_p, c_int],
         "cq_lnv_solve_host": [c_void_p, P(c_double), P(c_double), P(c_double), P(c_double), P(LNVResult)],
         "cq_lnv_reduction_log": [c_void_p, c_int, P(c_double), c_int64, P(c_int64)],
+        "cq_lnv_force_matrices": [c_void_p, c_void_p, c_void_p, c_int],
     }
     for name, args in lnv_sigs.items():
         f = getattr(L, name)
@@ -391,6 +392,13 @@ class LNV:
         n = c_int64()
         check(lib().cq_lnv_reduction_log(self._h, int(bool(enable)), _dp(out), cap, ctypes.byref(n)))
         return out[:min(n.value, cap)]
+
+    def force_matrices(self):
+        """(M12 in the S range, M4 in the H range) of the current L, as host arrays."""
+        M12 = np.zeros(self.system.length(self.range_ids["S"]))
+        M4 = np.zeros(self.system.length(self.range_ids["H"]))
+        check(lib().cq_lnv_force_matrices(self._h, M12.ctypes.data_as(c_void_p), M4.ctypes.data_as(c_void_p), 0))
+        return M12, M4
 
     def solve_host(self, S, H, want_L=False, want_K=False):
         S = np.ascontiguousarray(S, np.float64); H = np.ascontiguousarray(H, np.float64)

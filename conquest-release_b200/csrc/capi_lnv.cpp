@@ -179,6 +179,19 @@ int cq_lnv_solve_host(cq_lnv* s, const double* S, const double* H, double* L_out
   });
 }
 
+int cq_lnv_force_matrices(cq_lnv* s, double* M12, double* M4, int on_device) {
+  return guarded_call([&] {
+    CQ_CHECK(s, CQ_ERR_ARG, "null argument");
+    LNVSolver& L = *s->solver;
+    DMat m12 = L.temp(LNVSolver::RS), m4 = L.temp(LNVSolver::RH);
+    L.force_matrices(m12, m4);
+    const auto kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (M12) CQ_CUDA(cudaMemcpyAsync(M12, m12.p, sizeof(double) * m12.n, kind, L.S.stream));
+    if (M4) CQ_CUDA(cudaMemcpyAsync(M4, m4.p, sizeof(double) * m4.n, kind, L.S.stream));
+    CQ_CUDA(cudaStreamSynchronize(L.S.stream));
+  });
+}
+
 int cq_lnv_reduction_log(cq_lnv* s, int enable, double* out, int64_t cap, int64_t* n) {
   return guarded_call([&] {
     CQ_CHECK(s, CQ_ERR_ARG, "null argument");

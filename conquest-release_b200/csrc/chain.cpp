@@ -62,6 +62,8 @@ const LNVSolver::Mult LNVSolver::kMults[] = {
     {1, RT, RH, RTH},     // T_H_TH
     {1, RT, RL, RTL},     // T_L_TL
     {2, RL, RT, RTL},     // TL_T_L
+    {1, RLH, RL, RSLS},   // LH_L_SLS (type 1 while rcut(SLS) >= rcut(LH), mult_module.f90:660-680)
+    {2, RS, RLS, RSLS},   // LHL_SL_S (mult_module.f90:753-760)
 };
 
 void LNVSolver::product(const DMat& A, const DMat& B, DMat& C, MultId id) {
@@ -352,6 +354,32 @@ void LNVSolver::lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* p
   if (doE) *energy = t[0];
   if (dophi) *electrons = 3.0 * t[doE ? 1 : 0] - 2.0 * t[doE ? 2 : 1];
   stats.n_lnv++;
+}
+
+void LNVSolver::force_matrices(DMat& M12, DMat& M4) {
+  CQ_CHECK(M12.rng == RS && M4.rng == RH, CQ_ERR_STATE, "force matrices: M12 has the S range, M4 the H range");
+  CQ_CHECK(S.ranges[R[RSLS]]->rcut >= S.ranges[R[RLH]]->rcut, CQ_ERR_STATE,
+           "LH.L -> SLS is a type-1 product only while rcut(SLS) >= rcut(LH)");
+  const bool um = use_mixed;
+  use_mixed = false;
+  product(L, Smat, LS, L_S_LS);
+  transpose(LS, SL);
+  DMat LH = temp(RLH), LHL = temp(RSLS);
+  product(L, Hmat, LH, L_H_LH);
+  product(LH, L, LHL, LH_L_SLS);
+  DMat LHLSL = temp(RS), LSLHL = temp(RS);
+  product(LHL, LS, LHLSL, LHL_SL_S);
+  transpose(LHLSL, LSLHL);
+  ensure_workspace();
+  DMat& LSL = wA;
+  product(LS, L, LSL, LS_L_LSL);
+  product(LSL, LS, wLSLSL, LSL_SL_H);
+  msum(0.0, M4, 12.0, LSL);
+  msum(1.0, M4, -12.0, wLSLSL);
+  msum(0.0, M12, 3.0, LHL);
+  msum(1.0, M12, -2.0, LHLSL);
+  msum(1.0, M12, -2.0, LSLHL);
+  use_mixed = um;
 }
 
 void LNVSolver::symmetrise_L() {

@@ -48,7 +48,7 @@ class LNVSolver {
   // named ranges of the chain, in the order of cq_lnv_create's range list
   enum Rng { RS = 0, RH, RL, RT, RLS, RLH, RLSL, RSLS, RTS, RTH, RTL, NR };
   enum MultId { L_S_LS = 0, L_H_LH, T_S_TS, SL_S_SLS, LS_L_LSL, HL_S_LSL, HLS_LS_L, SLS_LS_L, LSL_SL_H, TS_T_T,
-                TH_T_L, T_H_TH, T_L_TL, TL_T_L };
+                TH_T_L, T_H_TH, T_L_TL, TL_T_L, LH_L_SLS, LHL_SL_S };
   struct Mult { int type, a, b, c; };
   static const Mult kMults[];
 
@@ -75,6 +75,9 @@ class LNVSolver {
   // split precision until the residual reaches prm.mixed_tolerance, then FindMinDM continues in FP64
   void solve();
   void purify(int sweeps);
+  // M12 (S range) and M4 (H range) of the current L: the doM1 + doM2 and doM4 branches of
+  // LNV_matrix_multiply, the density-matrix terms of the forces
+  void force_matrices(DMat& M12, DMat& M4);
   bool use_mixed = false;   // current product arithmetic of mult_dispatch
   static void do_pulay(int iPulay, const double* Aij, int n, int max_n, double* al);
   void lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim, double* electrons, double* energy);

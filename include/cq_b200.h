@@ -302,6 +302,14 @@ int cq_lnv_solve_host(cq_lnv* s, const double* S, const double* H, double* L_out
 int cq_exact_dots_noalloc(int count, const double* const* x_dev, const double* const* y_dev, const int64_t* n,
                           void* stream, double* out);
 
+/* Force matrices of the current L (the doM1 + doM2 and doM4 branches of LNV_matrix_multiply,
+ * src/mult_module.f90:1564-1592, 1680-1726), FP64 with the reference's rounding:
+ *   M12 = 3 LHL - 2 LHLSL - 2 LSLHL  (S range; LHL = LH.L in the SLS range, LHLSL = LHL.SL pruned
+ *                                      to the S range, LSLHL its transpose)
+ *   M4  = 12 LSL - 12 LSLSL          (H range)
+ * Either output may be NULL.  on_device: the outputs are device arrays. */
+int cq_lnv_force_matrices(cq_lnv* s, double* M12, double* M4, int on_device);
+
 /* Reduction log (tracing): with enable = 1 every later trace and product trace of the chain
  * (matrix_trace / matrix_product_trace values, in call order) is recorded.  Each call returns
  * the values recorded so far (*n of them, at most cap copied to out), clears the log and sets

@@ -42,6 +42,8 @@ MULTS = {
     "T_H_TH": (1, "T", "H", "TH"),
     "T_L_TL": (1, "T", "L", "TL"),
     "TL_T_L": (2, "L", "T", "TL"),
+    "LH_L_SLS": (1, "LH", "L", "SLS"),      # type 1 while rcut(SLS) >= rcut(LH) (mult_module.f90:660-680)
+    "LHL_SL_S": (2, "S", "LS", "SLS"),      # mult_module.f90:753-760
 }
 
 
@@ -269,7 +271,32 @@ class OracleLNV:
     def copy(self, A):
         return Mat(A.rng, A.v.copy())
 
-    # ---- LNV_matrix_multiply (doM3, dophi, doE, doK; doM1/doM2/doM4 unused by the chain) ----
+    # ---- force matrices: the doM1 + doM2 and doM4 branches of LNV_matrix_multiply ----------
+    def force_matrices(self):
+        """M12 = 3 LHL - 2 LHLSL - 2 LSLHL (S range) and M4 = 12 LSL - 12 LSLSL (H range) of the current
+        L (mult_module.f90:1564-1592, 1680-1726), the matrices the forces need from the density matrix."""
+        L, S, H = self.L, self.S, self.H
+        self.product(L, S, self.LS, "L_S_LS")
+        self.transpose(self.LS, self.SL)
+        LH = self.temp("LH")
+        self.product(L, H, LH, "L_H_LH")
+        LHL = self.temp("SLS")
+        self.product(LH, L, LHL, "LH_L_SLS")
+        LHLSL = self.temp("S"); LSLHL = self.temp("S")
+        self.product(LHL, self.LS, LHLSL, "LHL_SL_S")
+        self.transpose(LHLSL, LSLHL)
+        LSL = self.temp("LSL"); LSLSL = self.temp("H")
+        self.product(self.LS, L, LSL, "LS_L_LSL")
+        self.product(LSL, self.LS, LSLSL, "LSL_SL_H")
+        M12 = self.temp("S"); M4 = self.temp("H")
+        self.msum(0.0, M4, 12.0, LSL)
+        self.msum(1.0, M4, -12.0, LSLSL)
+        self.msum(0.0, M12, 3.0, LHL)
+        self.msum(1.0, M12, -2.0, LHLSL)
+        self.msum(1.0, M12, -2.0, LSLHL)
+        return M12.v, M4.v
+
+    # ---- LNV_matrix_multiply (doM3, dophi, doE, doK; doM1/doM2/doM4: force_matrices) ----
     def lnv(self, doK=False, doM3=False, dophi=False, doE=False, M3=None, phi=None):
         L, S, H = self.L, self.S, self.H
         electrons = energy = None

@@ -102,3 +102,21 @@ def test_graph_replay_matches_direct_launches():
     assert (r0["energy"], r0["electrons"], r0["n_products"]) == (r1["energy"], r1["electrons"], r1["n_products"])
     assert np.array_equal(L0, L1)
     assert hashlib.sha256(np.ascontiguousarray(L1, np.float64).tobytes()).hexdigest() == gold["L_sha256"]
+
+
+def test_force_matrices_match_oracle():
+    """M12 (S range) and M4 (H range) of a given L: the doM1 + doM2 and doM4 branches of
+    LNV_matrix_multiply, bit for bit against the oracle on the same L."""
+    coords, cell = inputs.diamond_si(2, sigma=0.1, seed=2)
+    n = len(coords)
+    o, g, ridx, S, H, olnv, glnv = _setup(coords, cell, np.full(n, 4), float(n), 8.0, 9.0, 10.0, 8.0)
+    glnv.set_SH(S, H)
+    rs = np.random.default_rng(17)
+    Lr = rs.uniform(-0.05, 0.05, g.length(ridx["L"]))
+    glnv.put("L", Lr)
+    olnv.L.v[:] = Lr
+    M12, M4 = glnv.force_matrices()
+    oM12, oM4 = olnv.force_matrices()
+    assert np.array_equal(M12, oM12)
+    assert np.array_equal(M4, oM4)
+    assert np.abs(M12).max() > 0 and np.abs(M4).max() > 0
