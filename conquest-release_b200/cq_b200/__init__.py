@@ -104,6 +104,8 @@ def lib():
         "cq_pulay_alphas": [c_int, P(c_double), c_int, c_int, P(c_double)],
         "cq_system_set_option": [c_void_p, c_int, c_int],
         "cq_generate_SH": [c_void_p, c_int, c_int, ctypes.c_uint64, c_void_p],
+        "cq_dump_matrix": [c_void_p, c_int, c_void_p, ctypes.c_char_p, c_int],
+        "cq_grab_matrix": [c_void_p, c_int, c_void_p, ctypes.c_char_p, P(c_int64)],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -283,6 +285,16 @@ class System:
     def generate_SH(self, r, which, seed, out):
         """Synthetic S (which=0) or H (which=1) of range r into the device array `out`, stream-ordered."""
         check(lib().cq_generate_SH(self._h, int(r), int(which), int(seed), _ptr(out)))
+
+    def dump_matrix(self, r, a, path, inode=1):
+        """Write the device array `a` of range r as a matrix file of the reference's binary format."""
+        check(lib().cq_dump_matrix(self._h, int(r), _ptr(a), os.fsencode(path), int(inode)))
+
+    def grab_matrix(self, r, a, path):
+        """Read a matrix file into the device array `a` of range r; returns the number of matched blocks."""
+        m = c_int64()
+        check(lib().cq_grab_matrix(self._h, int(r), _ptr(a), os.fsencode(path), ctypes.byref(m)))
+        return m.value
 
     def set_blocking_sync(self, on=True):
         """Host waits for device scalars sleep on a blocking-sync event (many solvers per core)."""

@@ -111,6 +111,18 @@ int cq_mat_mult(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a
 int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c,
                      int precision);
 
+/*
+ * Matrix files in the reference's binary format (dump_matrix2 / grab_matrix2,
+ * src/store_matrix_module.f90:340-430, 1199-1421: Fortran unformatted sequential records; one
+ * file per process, here one): the device array a_dev of range r is written with its block
+ * layout (global ids, neighbours' block sizes, fractional image vectors) or read back.  Reading
+ * matches every block of the file to a block of the range by (global i, global j, image vector);
+ * blocks of the range absent from the file become zero; *matched receives the number of matched
+ * file blocks.  Restart and persistence of L (`Lmatrix2` files).
+ */
+int cq_dump_matrix(cq_system* sys, int r, const double* a_dev, const char* path, int inode);
+int cq_grab_matrix(cq_system* sys, int r, double* a_dev, const char* path, int64_t* matched);
+
 /* Algorithmic work of one product: (k,i,j) triples with a stored result and 2*sum nd^3 flops. */
 int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* triples, int64_t* flops);
 
