@@ -21,7 +21,11 @@ c_int, c_double, c_void_p, c_int64 = ctypes.c_int, ctypes.c_double, ctypes.c_voi
 P = ctypes.POINTER
 
 # mirror of the status codes in include/cq_b200.h
-CQ_OK, CQ_ERR_ARG, CQ_ERR_OOM, CQ_ERR_CUDA, CQ_ERR_BOUNDS, CQ_ERR_TIMEOUT, CQ_ERR_STATE, CQ_ERR_NOT_CONVERGED = range(8)
+(CQ_OK, CQ_ERR_ARG, CQ_ERR_OOM, CQ_ERR_CUDA, CQ_ERR_BOUNDS, CQ_ERR_TIMEOUT, CQ_ERR_STATE, CQ_ERR_NOT_CONVERGED,
+ CQ_ERR_CALLBACK) = range(9)
+
+# cq_h_rebuild_fn: (user, K_dev, H_dev, length, stream) -> status
+H_REBUILD_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_void_p, c_void_p, c_int64, c_void_p)
 # product arithmetic (cq_mat_mult precision)
 PREC_FP64_FMA, PREC_FP64, PREC_BF16X3 = 0, 1, 2
 
@@ -404,6 +408,24 @@ class LNV:
         n = c_int64()
         check(lib().cq_lnv_reduction_log(self._h, int(bool(enable)), _dp(out), cap, ctypes.byref(n)))
         return out[:min(n.value, cap)]
+
+    def set_h_rebuild(self, fn):
+        """Mixed-L self-consistency (minE.MixedLSelfConsistent): lateDM calls fn(K_ptr, H_ptr, length,
+        stream) with the solver's device pointers of K and H (H range) at its start and after every
+        Pulay step; fn writes the new H into H_ptr, ordered on `stream`, and returns 0.  None
+        switches the coupling off."""
+        if fn is None:
+            self._h_cb = None
+            check(lib().cq_lnv_set_h_rebuild(self._h, H_REBUILD_FN(), None))
+            return
+
+        def tramp(user, k, h, n, stream):
+            try:
+                return int(fn(k or 0, h or 0, int(n), stream or 0))
+            except Exception:
+                return -1
+        self._h_cb = H_REBUILD_FN(tramp)      # kept alive while the solver may call it
+        check(lib().cq_lnv_set_h_rebuild(self._h, self._h_cb, None))
 
     def force_matrices(self):
         """(M12 in the S range, M4 in the H range) of the current L, as host arrays."""

@@ -203,4 +203,12 @@ int cq_lnv_reduction_log(cq_lnv* s, int enable, double* out, int64_t cap, int64_
   });
 }
 
+int cq_lnv_set_h_rebuild(cq_lnv* s, cq_h_rebuild_fn fn, void* user) {
+  return guarded_call([&] {
+    CQ_CHECK(s && s->solver, CQ_ERR_ARG, "null solver");
+    s->solver->h_rebuild = fn;
+    s->solver->h_rebuild_user = fn ? user : nullptr;
+  });
+}
+
 }  // extern "C"

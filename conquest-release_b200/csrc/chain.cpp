@@ -744,6 +744,7 @@ int LNVSolver::late_dm(int ndone, bool& done, double& deltaE) {
   DMat M3 = temp(RL), SM3 = temp(RL), Sphi = temp(RL), mtemp = temp(RTL);
   int iter_stuck = 0;
   double el, e0;
+  if (h_rebuild) rebuild_H();
   lnv(false, true, true, true, &M3, &phi, &el, &e0);
   double energy0 = 2.0 * e0;
   tmt(M3, SM3, mtemp, T);
@@ -804,6 +805,7 @@ int LNVSolver::late_dm(int ndone, bool& done, double& deltaE) {
     scale(0.0, L);
     for (int i = 0; i < pul_mx; ++i) msum(1.0, L, alph[i], Lst[i]);
     if (prm.vary_mu) correct_electron_number();
+    if (h_rebuild) rebuild_H();
     lnv(false, true, true, true, &M3, &phi, &el, &e1);
     double energy1 = 2.0 * e1;
     tmt(M3, SM3, mtemp, T);
@@ -816,7 +818,7 @@ int LNVSolver::late_dm(int ndone, bool& done, double& deltaE) {
     stats.last_energy = energy1;
     stats.last_residual = g1;
     if (g1 < prm.tolerance) { done = true; return n_iter; }
-    else if (g1 > 2.0 * g0) return n_iter;
+    else if (!h_rebuild && g1 > 2.0 * g0) return n_iter;   // no residual-rise exit with the H coupling
     else if (g1 > 0.99 * g0) {
       if (++iter_stuck > 5) return n_iter;
     }
@@ -827,6 +829,16 @@ int LNVSolver::late_dm(int ndone, bool& done, double& deltaE) {
     energy0 = energy1;
   }
   return ndone;
+}
+
+// Mixed-L self-consistency step of lateDM (DMMinModule.f90:894-907, 1138-1149): K and Tr(KH) of
+// the current L, then the caller rebuilds H from the density of K (get_electronic_density and
+// get_H_matrix in the reference).  H keeps its address, so captured LNV graphs stay valid.
+void LNVSolver::rebuild_H() {
+  double el = 0.0, e = 0.0;
+  lnv(true, false, false, true, nullptr, nullptr, &el, &e);
+  const int rc = h_rebuild(h_rebuild_user, K.p, Hmat.p, Hmat.n, (void*)S.stream);
+  CQ_CHECK(rc == 0, CQ_ERR_CALLBACK, "the H rebuild callback returned " + std::to_string(rc));
 }
 
 void LNVSolver::find_min_dm(bool resetL) {

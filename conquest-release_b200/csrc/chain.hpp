@@ -123,6 +123,12 @@ class LNVSolver {
   void project_gradient(DMat& M3, DMat& SM3, DMat& Sphi, DMat& mtemp);
   int early_dm(int ndone, bool& inflex);
   int late_dm(int ndone, bool& done, double& deltaE);
+ public:
+  // minE.MixedLSelfConsistent: the caller's density and H rebuild from K, run by lateDM
+  cq_h_rebuild_fn h_rebuild = nullptr;
+  void* h_rebuild_user = nullptr;
+ private:
+  void rebuild_H();
 };
 
 }  // namespace cqb

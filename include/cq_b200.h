@@ -36,6 +36,7 @@ extern "C" {
 #define CQ_ERR_TIMEOUT 5      /* a bounded wait ran out */
 #define CQ_ERR_STATE 6        /* call not valid in the current state */
 #define CQ_ERR_NOT_CONVERGED 7
+#define CQ_ERR_CALLBACK 8     /* a caller-supplied callback returned nonzero */
 
 typedef struct cq_system cq_system;
 
@@ -321,6 +322,22 @@ int cq_exact_dots_noalloc(int count, const double* const* x_dev, const double* c
  *   M4  = 12 LSL - 12 LSLSL          (H range)
  * Either output may be NULL.  on_device: the outputs are device arrays. */
 int cq_lnv_force_matrices(cq_lnv* s, double* M12, double* M4, int on_device);
+
+/*
+ * Mixed-L self-consistency (minE.MixedLSelfConsistent, src/DMMinModule.f90:894-907, 1138-1149):
+ * with a callback set, lateDM rebuilds H from the density of the current L at its start and after
+ * every Pulay step, as the reference does with get_electronic_density + get_H_matrix; the
+ * residual-rise exit of lateDM is then off (DMMinModule.f90:1261).  Each rebuild first evaluates
+ * K = 3LSL - 2LSLSL and Tr(KH) of the current L (LNV_matrix_multiply with doK, doE), then calls
+ *   fn(user, K_dev, H_dev, length, stream)
+ * on the solving thread: K_dev and H_dev are the solver's device arrays of K and H (both the H
+ * range, `length` doubles), `stream` is the solver's cudaStream_t.  The callback writes the new H
+ * into H_dev, in work enqueued on `stream` or finished before it returns, and returns 0; any other
+ * value ends the solve with CQ_ERR_CALLBACK.  It may call this library's matrix entry points on
+ * the solver's system (cq_matrix_sum and the like), not the cq_lnv_* entry points of this solver.
+ * fn = NULL switches the coupling off (the default). */
+typedef int (*cq_h_rebuild_fn)(void* user, const double* K_dev, double* H_dev, int64_t length, void* stream);
+int cq_lnv_set_h_rebuild(cq_lnv* s, cq_h_rebuild_fn fn, void* user);
 
 /* Reduction log (tracing): with enable = 1 every later trace and product trace of the chain
  * (matrix_trace / matrix_product_trace values, in call order) is recorded.  Each call returns

@@ -224,6 +224,9 @@ class OracleLNV:
         self.n_products = 0
         self.log = []
         self.rlog = []          # every trace / product-trace value in call order (chain comparison)
+        # minE.MixedLSelfConsistent: callable(K values) -> new H values, run by lateDM
+        self.h_rebuild = None
+        self.h_rebuilds = 0
 
     # ---- matrix layer (mult_module) -------------------------------------
     def temp(self, rng):
@@ -723,6 +726,8 @@ class OracleLNV:
         SGst = [self.temp("L") for _ in range(npul)]
         M3 = self.temp("L"); SM3 = self.temp("L"); Sphi = self.temp("L"); mat_temp = self.temp("TL")
         iter_stuck = 0
+        if self.h_rebuild is not None:
+            self.rebuild_H()
         electrons, e0 = self.lnv(doM3=True, dophi=True, doE=True, M3=M3, phi=self.phi)
         energy0 = sf * e0
         self.TMT(M3, SM3, mat_temp, self.T)
@@ -775,6 +780,8 @@ class OracleLNV:
                 self.msum(1.0, self.L, alph[i], Lst[i])
             if p.vary_mu:
                 self.correct_electron_number()
+            if self.h_rebuild is not None:
+                self.rebuild_H()
             electrons, e1 = self.lnv(doM3=True, dophi=True, doE=True, M3=M3, phi=self.phi)
             energy1 = sf * e1
             self.TMT(M3, SM3, mat_temp, self.T)
@@ -785,7 +792,7 @@ class OracleLNV:
             self.log.append(("lateDM", n_iter, energy1, g1))
             if g1 < p.tolerance:
                 return n_iter, True, deltaE
-            elif g1 > 2.0 * g0:
+            elif self.h_rebuild is None and g1 > 2.0 * g0:     # off with the H coupling (1261)
                 return n_iter, False, deltaE
             elif g1 > 0.99 * g0:
                 iter_stuck += 1
@@ -797,6 +804,13 @@ class OracleLNV:
             g0 = g1
             energy0 = energy1
         return p.n_L_iterations, done, deltaE
+
+    def rebuild_H(self):
+        """Mixed-L self-consistency step (DMMinModule.f90:894-907, 1138-1149): K and E of the
+        current L (LNV_matrix_multiply with doK, doE), then H from the density of K."""
+        self.lnv(doK=True, doE=True)
+        self.h_rebuilds += 1
+        self.H.v[:] = np.asarray(self.h_rebuild(self.K.v.copy()), dtype=np.float64)
 
     @staticmethod
     def do_pulay(iPulay, Aij_in, n, max_n, use_lapack=False):

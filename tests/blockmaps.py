@@ -115,3 +115,13 @@ def kat_transpose(bl, a):
         A = a[bl.elem_off[q]:bl.elem_off[q] + ndI * ndJ].reshape(ndJ, ndI).T
         at[off:off + ndJ * ndI] = A.ravel()  # A row-major is A^T column-major
     return at
+
+
+def dense(bl, v, n, nd):
+    """Dense (n nd) x (n nd) matrix of a range's values v (blocks of a cluster with no periodic images
+    in range; image blocks of one pair would be summed)."""
+    M = np.zeros((n * nd, n * nd))
+    for q in range(len(bl.ig_i)):
+        i, j = bl.ig_i[q], bl.ig_j[q]
+        M[i * nd:(i + 1) * nd, j * nd:(j + 1) * nd] += v[bl.elem_off[q]:bl.elem_off[q] + nd * nd].reshape(nd, nd).T
+    return M

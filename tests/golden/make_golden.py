@@ -7,6 +7,13 @@ T = S^-1, then FindMinDM from the McWeeny start) is run on the seeded synthetic 
 band energy, electron count, number of products and a SHA-256 of the final L (the raw float64
 bytes in the storage order of the oracle, which is the storage order of the library) are written
 to lnv_chain_si64.json (with the pass limit and whether the chain converged).  The GPU tests compare against these numbers bit for bit.
+
+lnv_scf_si64.json holds the same quantities for the chain with mixed-L self-consistency
+(minE.MixedLSelfConsistent): lateDM rebuilds H = H0 + g K from K of the current L at its start and
+after every Pulay step, a linear density feedback standing in for the grid rebuild of H, plus the
+number of rebuilds and a SHA-256 of the final H.
+
+    python tests/golden/make_golden.py [chain|scf]      (default: both)
 """
 import hashlib
 import json
@@ -28,7 +35,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 CASES = {"r8_9_10_8": ((8.0, 9.0, 10.0, 8.0), 2), "r10_12_16_10": ((10.0, 12.0, 16.0, 10.0), 40)}
 
 
-def run_case(ranges, max_outer):
+def run_case(ranges, max_outer, feedback=None):
     import blockmaps as bm
     import cq_b200
     from cq_b200 import inputs
@@ -42,15 +49,36 @@ def run_case(ranges, max_outer):
     S = inputs.overlap_S(bm.oracle_blocklist(o, ridx["S"], coords, cell))
     H = inputs.hamiltonian_H(bm.oracle_blocklist(o, ridx["H"], coords, cell), seed=5)
     lnv = OracleLNV(o, ridx, S, H, float(n), 4.0 * n, Params())
+    extra = {}
+    if feedback is not None:
+        H0 = np.array(H, dtype=np.float64)
+        lnv.h_rebuild = lambda K: H0 + feedback * K
     lnv.iter_hott_invs()
     E, N = lnv.find_min_dm(max_outer=max_outer)
-    return {"ranges": list(ranges), "max_outer": max_outer, "converged": bool(lnv.converged), "atoms": n, "ne_spin": float(n), "energy": E, "electrons": N,
+    if feedback is not None:
+        extra = {"feedback": feedback, "h_rebuilds": int(lnv.h_rebuilds),
+                 "H_sha256": hashlib.sha256(np.ascontiguousarray(lnv.H.v, np.float64).tobytes()).hexdigest()}
+    return {**extra,"ranges": list(ranges), "max_outer": max_outer, "converged": bool(lnv.converged), "atoms": n, "ne_spin": float(n), "energy": E, "electrons": N,
             "n_products": int(lnv.n_products),
             "L_sha256": hashlib.sha256(np.ascontiguousarray(lnv.L.v, np.float64).tobytes()).hexdigest(),
             "L_length": int(lnv.L.v.size)}
 
 
-def main():
+# name: (S, H, L, T ranges, pass limit, feedback g of H = H0 + g K)
+SCF_CASES = {"r8_9_10_8_gm005": ((8.0, 9.0, 10.0, 8.0), 1, -0.05)}
+
+
+def main(which=("chain", "scf")):
+    if "scf" in which:
+        out = {"system": "diamond Si 2x2x2 cells (64 atoms), sigma 0.1 bohr, seed 2; S overlap_S, H0 hamiltonian_H "
+                         "seed 5; 4x4 blocks; ne_spin = 64; H = H0 + g K rebuilt by lateDM", "cases": {}}
+        for name, (rg, mo, gfb) in SCF_CASES.items():
+            t = time.time()
+            out["cases"][name] = run_case(rg, mo, gfb)
+            print(name, out["cases"][name]["energy"], "%.1f s" % (time.time() - t), flush=True)
+        json.dump(out, open(os.path.join(HERE, "lnv_scf_si64.json"), "w"), indent=1)
+    if "chain" not in which:
+        return
     out = {"system": "diamond Si 2x2x2 cells (64 atoms), sigma 0.1 bohr, seed 2; S overlap_S, H hamiltonian_H seed 5; "
                      "4x4 blocks; ne_spin = 64", "cases": {}}
     for name, (rg, mo) in CASES.items():
@@ -61,4 +89,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]) or ("chain", "scf"))

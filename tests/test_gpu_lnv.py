@@ -36,12 +36,7 @@ def _setup(coords, cell, nsf, ne_spin, rs=10.0, rh=12.0, rl=16.0, rt=10.0, **par
     return o, g, ridx, S, H, olnv, glnv
 
 
-def _dense(bl, v, n, nd):
-    M = np.zeros((n * nd, n * nd))
-    for q in range(len(bl.ig_i)):
-        i, j = bl.ig_i[q], bl.ig_j[q]
-        M[i * nd:(i + 1) * nd, j * nd:(j + 1) * nd] += v[bl.elem_off[q]:bl.elem_off[q] + nd * nd].reshape(nd, nd).T
-    return M
+_dense = bm.dense
 
 
 def test_cluster_matches_dense_eigh():
@@ -163,3 +158,62 @@ def test_matrix_file_round_trip(tmp_path):
     matched = g.grab_matrix(rl, back, path)
     assert matched == g.n_blocks(rl)
     assert np.array_equal(back.cpu().numpy(), L)
+
+
+GOLDEN_SCF = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "lnv_scf_si64.json")))
+
+
+@pytest.mark.parametrize("case", sorted(GOLDEN_SCF["cases"]))
+def test_mixed_l_self_consistency_matches_oracle(case):
+    """lateDM with the H rebuild callback (mixed-L self-consistency): H = H0 + g K rebuilt on the
+    device through cq_matrix_sum at lateDM's start and after every Pulay step.  The same number
+    of rebuilds as the oracle chain, L and the final H to the bit, E and Ne within 1e-10."""
+    import torch
+    gold = GOLDEN_SCF["cases"][case]
+    coords, cell = inputs.diamond_si(2, sigma=0.1, seed=2)
+    n = len(coords)
+    o, g, ridx, S, H, olnv, glnv = _setup(coords, cell, np.full(n, 4), float(n), *gold["ranges"],
+                                          max_outer=gold["max_outer"])
+    rH = ridx["H"]
+    H0 = torch.tensor(H, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    calls = []
+
+    def rebuild(k, h, length, stream):
+        calls.append(length)
+        g.matrix_sum(rH, h, 0.0, rH, H0.data_ptr(), 1.0)
+        g.matrix_sum(rH, h, 1.0, rH, k, gold["feedback"])
+        return 0
+
+    glnv.set_h_rebuild(rebuild)
+    glnv.set_SH(S, H)
+    res = glnv.solve()
+    L, Hf = glnv.get("L"), glnv.get("H")
+    assert len(calls) == gold["h_rebuilds"] and set(calls) == {g.length(rH)}
+    assert res["converged"] == int(gold["converged"])
+    assert res["n_products"] == gold["n_products"]
+    assert abs(res["energy"] - gold["energy"]) <= 1e-10 * max(1.0, abs(gold["energy"]))
+    assert abs(res["electrons"] - gold["electrons"]) <= 1e-10 * max(1.0, abs(gold["electrons"]))
+    assert hashlib.sha256(np.ascontiguousarray(L, np.float64).tobytes()).hexdigest() == gold["L_sha256"]
+    assert hashlib.sha256(np.ascontiguousarray(Hf, np.float64).tobytes()).hexdigest() == gold["H_sha256"]
+
+
+def test_failing_h_rebuild_ends_the_solve_and_leaves_the_solver_usable():
+    """A nonzero status from the callback ends the solve with CQ_ERR_CALLBACK; with the coupling
+    switched off the same solver then reproduces the plain chain's fixture."""
+    import cq_b200
+    gold = GOLDEN["cases"]["r8_9_10_8"]
+    coords, cell = inputs.diamond_si(2, sigma=0.1, seed=2)
+    n = len(coords)
+    o, g, ridx, S, H, olnv, glnv = _setup(coords, cell, np.full(n, 4), float(n), *gold["ranges"],
+                                          max_outer=gold["max_outer"])
+    glnv.set_h_rebuild(lambda k, h, length, stream: 3)
+    glnv.set_SH(S, H)
+    with pytest.raises(cq_b200.CQError) as err:
+        glnv.solve()
+    assert err.value.code == cq_b200.CQ_ERR_CALLBACK
+    glnv.set_h_rebuild(None)
+    res = glnv.solve()
+    L = glnv.get("L")
+    assert res["n_products"] == gold["n_products"]
+    assert hashlib.sha256(np.ascontiguousarray(L, np.float64).tobytes()).hexdigest() == gold["L_sha256"]
