@@ -267,7 +267,7 @@ def main():
                          "many systems on concurrent slots vs the FP64 path one at a time; mult216 / mult512: single "
                          "block products (216-atom DZP C=A.B; the products of one 512-atom LNV call)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3"])
-    ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (-1 autotuned, 0..3)")
+    ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (-1 autotuned, 0..3, 5)")
     ap.add_argument("--one-solve", action="store_true",
                     help="run exactly one solve of the workload and print its result (for launch lists under ncu)")
     ap.add_argument("--requests", type=int, default=32)

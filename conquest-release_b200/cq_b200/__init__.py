@@ -178,6 +178,9 @@ class System:
         self._h = h
         self.n_atoms = coords.shape[0]
         self.rcuts = [float(x) for x in rcuts]
+        # handles of the LNV solvers built on this system: close() destroys them first, whatever
+        # order the garbage collector finalises the Python objects in
+        self._lnvs = set()
 
     @property
     def handle(self):
@@ -185,6 +188,9 @@ class System:
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
+            for h in list(getattr(self, "_lnvs", ())):
+                lib().cq_lnv_destroy(c_void_p(h))
+            self._lnvs = set()
             lib().cq_system_destroy(self._h)
             self._h = c_void_p()
 
@@ -239,11 +245,11 @@ class System:
         """FP64: (variant chosen by the autotuner or -1, {variant: timed ms}); mixed=True: (output blocks per
         warp chosen for the split-precision kernel or -1, {group size: timed ms})."""
         v, g = c_int(), c_int()
-        ms, gms = (ctypes.c_float * 5)(), (ctypes.c_float * 4)()
+        ms, gms = (ctypes.c_float * 6)(), (ctypes.c_float * 4)()
         check(lib().cq_product_tuning(self._h, mult_type, ra, rb, rc, ctypes.byref(v), ms, ctypes.byref(g), gms))
         if mixed:
             return g.value, {gs: gms[i] for i, gs in enumerate((1, 2, 4, 8)) if gms[i] > 0}
-        return v.value, {i: ms[i] for i in range(5) if ms[i] > 0}
+        return v.value, {i: ms[i] for i in range(6) if ms[i] > 0}
 
     def matrix_sum(self, ra, a, alpha, rb, b, beta):
         check(lib().cq_matrix_sum(self._h, ra, _ptr(a), float(alpha), rb, _ptr(b), float(beta)))
@@ -356,11 +362,15 @@ class LNV:
         h = c_void_p()
         check(lib().cq_lnv_create(system.handle, ids, float(ne_spin), ctypes.byref(self._p), ctypes.byref(h)))
         self._h = h
+        system._lnvs.add(h.value)
         self.range_ids = dict(range_ids)
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
-            lib().cq_lnv_destroy(self._h)
+            # destroyed here unless the system's close() has already destroyed it
+            if self._h.value in self.system._lnvs:
+                self.system._lnvs.discard(self._h.value)
+                lib().cq_lnv_destroy(self._h)
             self._h = c_void_p()
 
     def __del__(self):

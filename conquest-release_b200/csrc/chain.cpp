@@ -218,6 +218,7 @@ LNVSolver::LNVSolver(System& sys, const int ranges[NR], double ne_spin, const cq
   ni_in_cell = S.geo.n_atoms;
   Smat = own(RS); Hmat = own(RH); L = own(RL); T = own(RT); Ttran = own(RT);
   LS = own(RLS); SL = own(RLS); K = own(RH); phi = own(RL);
+  ++S.n_solvers;                  // last: a constructor that throws leaves the count unchanged
 }
 
 DMat LNVSolver::own(int rng) {
@@ -293,6 +294,7 @@ int LNVSolver::lnv_body(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMa
 
 LNVSolver::~LNVSolver() {
   for (auto& g : graphs_) if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
+  --S.n_solvers;
 }
 
 // One LNV_matrix_multiply call.  With prm.graphs, the first call with a given set of operands runs

@@ -207,7 +207,7 @@ struct ProductPlan {
   DevBuf<int4> tiles;
   DevBuf<int> order;              // output blocks by descending pair count (warp-staged 4x4 kernel)
   int tuned = -1;                 // FP64 kernel variant chosen by the autotuner (-1: not tuned yet)
-  float tune_ms[5] = {0, 0, 0, 0, 0};
+  float tune_ms[6] = {0, 0, 0, 0, 0, 0};
 };
 
 // Split-precision tensor-core product: pair lists sorted by the first operand block,
@@ -260,6 +260,7 @@ struct System {
   std::map<std::pair<int, int>, FragBuf> frags;   // (range, slot) fragment buffers of the mixed products
   cudaStream_t stream = nullptr;  // the stream all work of the system is enqueued on
   int uniform_nsf = 0;            // block size when every atom has the same one, else 0
+  int n_solvers = 0;              // live LNV solvers built on this system (destroyed before it)
   int max_nsf = 0;                // largest block size
   DevBuf<double> red_scratch;     // scratch of the min/max reductions
   DevBuf<uint64_t> acc_part;      // 192-bit partials of the exact sums

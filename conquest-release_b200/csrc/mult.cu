@@ -338,6 +338,78 @@ __global__ void __launch_bounds__(128, 5) k_mult_nd4_warp(MultArgs M, const int*
   }
 }
 
+// Uniform 4 x 4 blocks, four lanes per output block: lane m of a quad owns column m of the block
+// (elements n1 + 4m, n1 = 0..3).  At each step the quad takes the next pair of its list: its lanes
+// load the first-operand block with two coalesced 16-byte loads each into shared memory, all four
+// read the whole block back (broadcast), and each lane loads the four B values of its column
+// straight into registers.  Four times the lanes of k_mult_nd4_warp, for products with few output
+// blocks and long pair lists (type 2 into the H and L ranges).  Every element keeps the order of
+// its terms, so the results are the same bits.
+template <int TYPE, bool EXACT>
+__global__ void __launch_bounds__(128, 8) k_mult_nd4_quad(MultArgs M, const int* __restrict__ order) {
+  constexpr int kStride = 9;                     // double2 per staged block (8 + 1 padding)
+  __shared__ double2 sx[4][8 * kStride];
+  const unsigned kFull = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qd = lane >> 2, m = lane & 3;
+  const int base = (blockIdx.x * 4 + warp) * 8;  // first output slot of this warp
+  if (base >= M.n_out) return;                   // whole warp
+  const int slot = base + qd;
+  const bool has = slot < M.n_out;
+  const int q = has ? order[slot] : 0;
+  int64_t t = has ? M.ptr[q] : 0;
+  const int64_t tend = has ? M.ptr[q + 1] : 0;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  double2* X = sx[warp] + qd * kStride;          // this quad's staged block
+  const double2* Xg = reinterpret_cast<const double2*>(M.x);
+  const double2* Bg = reinterpret_cast<const double2*>(M.b);
+  int2 pr_next = t < tend ? M.pairs[t] : make_int2(-1, -1);   // pair of the next step, loaded a step ahead
+  while (__any_sync(kFull, t < tend)) {
+    const bool act = t < tend;                   // uniform over the quad
+    const int2 pr = pr_next;
+    pr_next = t + 1 < tend ? M.pairs[t + 1] : make_int2(-1, -1);
+    double bc[4];
+    if (act) {
+      X[m] = __ldg(Xg + (int64_t)pr.x * 8 + m);
+      X[m + 4] = __ldg(Xg + (int64_t)pr.x * 8 + m + 4);
+      if (TYPE == 1) {
+        // B[n3 + 4m], n3 = 0..3: the four contiguous values of column m
+        const double2 u = __ldg(Bg + (int64_t)pr.y * 8 + 2 * m), v = __ldg(Bg + (int64_t)pr.y * 8 + 2 * m + 1);
+        bc[0] = u.x; bc[1] = u.y; bc[2] = v.x; bc[3] = v.y;
+      } else {
+        // B[m + 4 n2], n2 = 0..3: for each n2 the quad reads one 32-byte sector
+        const double* Bb = M.b + (int64_t)pr.y * 16 + m;
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) bc[n2] = __ldg(Bb + 4 * n2);
+      }
+    }
+    __syncwarp();
+    if (act) {
+      double x[16];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {
+        const double2 xv = X[v];
+        x[2 * v] = xv.x; x[2 * v + 1] = xv.y;
+      }
+      // type 1: acc[n1] += sum_n3 x[n1 + 4 n3] B[n3 + 4m]; type 2: acc[n1] += sum_n2 x[n1 + 4 n2] B[m + 4 n2]
+#pragma unroll
+      for (int n1 = 0; n1 < 4; ++n1) {
+        double a = acc[n1];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) a = madd<EXACT>(a, x[n1 + 4 * n], bc[n]);
+        acc[n1] = a;
+      }
+      ++t;
+    }
+    __syncwarp();
+  }
+  if (has) {
+    double2* O2 = reinterpret_cast<double2*>(M.out + 16 * (int64_t)q) + 2 * m;
+    O2[0] = make_double2(acc[0], acc[1]);
+    O2[1] = make_double2(acc[2], acc[3]);
+  }
+}
+
 // Any block sizes up to 16 (DZP 13 x 13, mixed SZ/DZP): one warp per output block, each lane a
 // 4 x 2 register tile of the output block (rows 4rt..4rt+3, columns 2ct..2ct+1, lane = rt * nct + ct),
 // so per term of the inner sum a lane loads 4 + 2 operand values for 8 multiply-adds instead of
@@ -448,7 +520,7 @@ void launch_dropin(int type, const int64_t* d_out, const int* d_dims, const int6
   CQ_CUDA(cudaGetLastError());
 }
 
-// One launch of the FP64 product with kernel `variant` (0..3 for uniform 4 x 4 blocks with
+// One launch of the FP64 product with kernel `variant` (0..3 and 5 for uniform 4 x 4 blocks with
 // 16-byte aligned operands; anything else runs the generic kernel).  All variants give the same
 // bits: they differ only in how the work is mapped onto the GPU.
 static void launch_variant(System& S, ProductPlan& P, const MultArgs& M, int variant, int exact, bool nd4) {
@@ -456,15 +528,24 @@ static void launch_variant(System& S, ProductPlan& P, const MultArgs& M, int var
   const int T = 256;
   RangeIndex& O = P.mult_type == 1 ? *S.ranges[P.rc] : *S.ranges[P.ra];
   RangeIndex& X = P.mult_type == 1 ? *S.ranges[P.ra] : *S.ranges[P.rc];
-  if (nd4 && variant == 3) {
-    if (P.order.n == 0) {
-      // output blocks by descending pair count (stable): lanes of a warp get similar list lengths
-      std::vector<int64_t> ptr = P.ptr.download(st);
-      std::vector<int> ord(M.n_out);
-      std::iota(ord.begin(), ord.end(), 0);
-      std::stable_sort(ord.begin(), ord.end(), [&](int u, int v) { return ptr[u + 1] - ptr[u] > ptr[v + 1] - ptr[v]; });
-      P.order.upload(ord, st);
+  if (nd4 && (variant == 3 || variant == 5) && P.order.n == 0) {
+    // output blocks by descending pair count (stable): lanes of a warp get similar list lengths
+    std::vector<int64_t> ptr = P.ptr.download(st);
+    std::vector<int> ord(M.n_out);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int u, int v) { return ptr[u + 1] - ptr[u] > ptr[v + 1] - ptr[v]; });
+    P.order.upload(ord, st);
+  }
+  if (nd4 && variant == 5) {
+    const int grid = (M.n_out + 31) / 32;        // 8 output blocks per warp, 4 warps per CTA
+    if (P.mult_type == 1) {
+      if (exact) k_mult_nd4_quad<1, true><<<grid, 128, 0, st>>>(M, P.order.p);
+      else k_mult_nd4_quad<1, false><<<grid, 128, 0, st>>>(M, P.order.p);
+    } else {
+      if (exact) k_mult_nd4_quad<2, true><<<grid, 128, 0, st>>>(M, P.order.p);
+      else k_mult_nd4_quad<2, false><<<grid, 128, 0, st>>>(M, P.order.p);
     }
+  } else if (nd4 && variant == 3) {
     const int grid = (M.n_out + 127) / 128;
     if (P.mult_type == 1) {
       if (exact) k_mult_nd4_warp<1, true><<<grid, 128, 0, st>>>(M, P.order.p);
@@ -533,17 +614,17 @@ static void launch_variant(System& S, ProductPlan& P, const MultArgs& M, int var
 // leaves the correct result.
 static int tuned_variant(System& S, ProductPlan& P, const MultArgs& M, int exact, bool nd4) {
   if (P.tuned >= 0) return P.tuned;
-  // candidates, the preferred kernel first: uniform 4x4 blocks: warp-staged, thread per block,
-  // 16 lanes per block (the most parallel, for products with few output blocks); other sizes:
-  // register-tiled, generic
-  int cands[3];
+  // candidates, the preferred kernel first: uniform 4x4 blocks: warp-staged, four lanes per
+  // block, thread per block, 16 lanes per block (the last two the most parallel, for products with
+  // few output blocks); other sizes: register-tiled, generic
+  int cands[4];
   int nc = 0;
-  if (nd4) { cands[0] = 3; cands[1] = 1; cands[2] = 0; nc = 3; }
+  if (nd4) { cands[0] = 3; cands[1] = 5; cands[2] = 1; cands[3] = 0; nc = 4; }
   else { cands[0] = 4; cands[1] = 0; nc = 2; }
   cudaEvent_t e0, e1;
   CQ_CUDA(cudaEventCreate(&e0));
   CQ_CUDA(cudaEventCreate(&e1));
-  float best[3] = {1e30f, 1e30f, 1e30f};
+  float best[4] = {1e30f, 1e30f, 1e30f, 1e30f};
   for (int c = 0; c < nc; ++c) launch_variant(S, P, M, cands[c], exact, nd4);
   for (int round = 0; round < 3; ++round)
     for (int c = 0; c < nc; ++c) {

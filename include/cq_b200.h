@@ -65,6 +65,8 @@ const char* cq_version(void);
 int cq_system_create(int n_atoms, const double* coords, const double* cell, const int* nsf, int n_ranges,
                      const double* rcuts, int max_atoms_part, double gap_threshold, double avg_atomic_diameter,
                      cq_system** out);
+/* Fails with CQ_ERR_STATE, destroying nothing, while LNV solvers built on the system are alive:
+ * destroy those (cq_lnv_destroy) first. */
 int cq_system_destroy(cq_system* sys);
 
 /* Number of stored elements (mat_p(A)%length) and blocks of range r. */
@@ -128,7 +130,7 @@ int cq_grab_matrix(cq_system* sys, int r, double* a_dev, const char* path, int64
 int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* triples, int64_t* flops);
 
 /* Autotuner record of one product: the FP64 kernel variant it chose (-1 before the product's
- * first autotuned call) and the timed milliseconds of each candidate variant (ms[5], 0 = not
+ * first autotuned call) and the timed milliseconds of each candidate variant (ms[6], 0 = not
  * timed); for its split-precision form the output blocks per warp it chose (1, 2, 4 or 8; -1 =
  * not tuned yet) and the timed milliseconds of those four group sizes (group_ms[4]). */
 int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int* variant, float* ms, int* group,
@@ -197,9 +199,11 @@ int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out)
  * events and keeps the fastest), 0 = one lane per output element, 1 = one thread per output
  * block, 2 = one thread per output block with the first operand's row staged in shared memory,
  * 3 = one thread per output block with the warp staging the operand blocks through shared
- * memory; for other block sizes (DZP 13 x 13, mixed sizes) 0 = one warp per output block, one lane
- * per element, 4 = one warp per output block, a 4 x 2 register tile per lane (the autotuner
- * candidates are 3/1/0 for uniform 4 x 4 blocks and 4/0 otherwise).  All give identical results.
+ * memory, 5 = four lanes per output block (one column each), the first operand's block staged
+ * in shared memory; for other block sizes (DZP 13 x 13, mixed sizes) 0 = one warp per output
+ * block, one lane per element, 4 = one warp per output block, a 4 x 2 register tile per lane (the
+ * autotuner candidates are 3/5/1/0 for uniform 4 x 4 blocks and 4/0 otherwise).  All give
+ * identical results.
  * CQ_OPT_BLOCKING_SYNC: 1 = the host thread sleeps on a blocking-sync event whenever the
  * solver waits for a scalar from the device (many concurrent solvers per host core), 0 = it
  * spins in cudaStreamSynchronize (default, lowest latency for one solver). */

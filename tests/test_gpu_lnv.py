@@ -217,3 +217,20 @@ def test_failing_h_rebuild_ends_the_solve_and_leaves_the_solver_usable():
     L = glnv.get("L")
     assert res["n_products"] == gold["n_products"]
     assert hashlib.sha256(np.ascontiguousarray(L, np.float64).tobytes()).hexdigest() == gold["L_sha256"]
+
+
+def test_system_outlives_its_solvers():
+    """cq_system_destroy refuses while a solver of the system is alive; System.close() destroys the
+    system's solvers first, so finalising the Python objects in either order is safe."""
+    import ctypes
+    import cq_b200
+    coords, cell = inputs.diamond_si(1, sigma=0.1, seed=2)
+    n = len(coords)
+    o, g, ridx, S, H, olnv, glnv = _setup(coords, cell, np.full(n, 4), float(n), 8.0, 9.0, 10.0, 8.0)
+    glnv.set_SH(S, H)
+    assert cq_b200.lib().cq_system_destroy(g.handle) == cq_b200.CQ_ERR_STATE
+    assert g.length(ridx["L"]) > 0                  # the system is untouched
+    g.close()                                       # destroys the solver, then the system
+    assert not g.handle.value
+    glnv.close()                                    # nothing left to destroy
+    assert not glnv._h.value
