@@ -405,7 +405,7 @@ def main():
                       "flops": per_solve_flops, "late_iters": res["late_iters"], "early_iters": res["early_iters"],
                       "mcw_sweeps": res["mcw_sweeps"], "converged": res["converged"]},
             "block_mult_tflops": (prof["flops"] / (prof["ms"] / 1e3) / 1e12) if prof["ms"] > 0 else None,
-            "roofline": {"bound": "hbm", "kernel": "FP64 4x4 block products (autotuned k_mult_nd4_warp / k_mult_nd4_tpb)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "FP64 4x4 block products (autotuned k_mult_nd4_warp / k_mult_nd4_quad)", "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "launches": prof["launches"],
                          "avg_launch_ms": prof["ms"] / max(1, prof["launches"]),
