@@ -268,6 +268,8 @@ def main():
                          "block products (216-atom DZP C=A.B; the products of one 512-atom LNV call)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3"])
     ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (-1 autotuned, 0..3, 5)")
+    ap.add_argument("--work-record", default=None,
+                    help="write the workload's per-solve work (flops, products, energy) as JSON to this path")
     ap.add_argument("--one-solve", action="store_true",
                     help="run exactly one solve of the workload and print its result (for launch lists under ncu)")
     ap.add_argument("--requests", type=int, default=32)
@@ -380,8 +382,9 @@ def main():
         fl_call = flops_of_lnv_call(system, prob["ridx"])
         rec = {"workload": WORKLOAD, "flops_per_solve": per_solve_flops, "products_per_solve": res["n_products"],
                "flops_per_lnv_call": fl_call, "energy": res["energy"], "electrons": res["electrons"]}
-        os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-        json.dump(rec, open(os.path.join(ROOT, "gpurun_out", "lnv512_solve_work.json"), "w"), indent=1)
+        if args.work_record:
+            os.makedirs(os.path.dirname(os.path.abspath(args.work_record)), exist_ok=True)
+            json.dump(rec, open(args.work_record, "w"), indent=1)
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
             nth = os.cpu_count() or 1

@@ -1,6 +1,6 @@
 """GPU LNV / McWeeny chain vs the oracle chain and vs the exact dense answer.
 
-Tolerances (north star): band energy and electron count within 1e-10 of the
+Tolerances: band energy and electron count within 1e-10 of the
 oracle for the FP64 path.
 """
 import hashlib
