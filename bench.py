@@ -132,14 +132,17 @@ def fp64_peak_tflops(dev):
 
 
 def load_traffic():
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary (None if absent)."""
+    """DRAM bytes of one captured launch of the dominant kernel, from the committed ncu summary:
+    (bytes, description of the launch, its algorithmic bytes), or (None, None, None) if absent."""
     p = os.path.join(ROOT, "profiles", "lnv512_mult_traffic.json")
     if os.path.exists(p):
         try:
-            return json.load(open(p)).get("dram_bytes_per_launch")
+            d = json.load(open(p))
+            return (d.get("dram_bytes_per_launch"), "%s on %s" % (d.get("kernel"), d.get("launch")),
+                    d.get("algorithmic_bytes_of_launch"))
         except Exception:
-            return None
-    return None
+            pass
+    return None, None, None
 
 
 def work_record_path():
@@ -410,7 +413,8 @@ def main():
             "block_mult_tflops": (prof["flops"] / (prof["ms"] / 1e3) / 1e12) if prof["ms"] > 0 else None,
             "roofline": {"bound": "hbm", "kernel": "FP64 4x4 block products (autotuned k_mult_nd4_warp / k_mult_nd4_quad)", "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "launches": prof["launches"],
+                         "traffic": traffic[0], "traffic_launch": traffic[1],
+                         "traffic_launch_algorithmic_bytes": traffic[2], "launches": prof["launches"],
                          "avg_launch_ms": prof["ms"] / max(1, prof["launches"]),
                          "algorithmic_bytes_per_launch": prof["bytes"] / max(1, prof["launches"]),
                          "share_of_step": prof["ms"] / prof_step_ms if prof_step_ms > 0 else None,
