@@ -44,3 +44,36 @@ def test_mcweeny_start_is_the_ground_state_density():
     ev = sla.eigh(Hd, Sd, eigvals_only=True)
     exact = 2.0 * ev[:n].sum()
     assert abs(2.0 * np.trace(Ld @ Hd) - exact) < 1e-10 * abs(exact)
+
+
+def test_solve_cubic_roots():
+    """SolveCubic (DMMinModule.f90:2072-2143): a real root of x^3 + a x^2 + b x + c; with three real
+    roots the one of least magnitude.  Cardano's formula loses a few digits where its two cube
+    roots cancel, so roots are compared at 1e-6 relative."""
+    rs = np.random.default_rng(1)
+    for _ in range(2000):
+        a, b, c = rs.normal(size=3) * rs.choice([0.1, 1.0, 10.0], 3)
+        x = OracleLNV.solve_cubic(a, b, c, 1.0e6)
+        r = np.roots([1.0, a, b, c])
+        real = r[np.abs(r.imag) < 1e-9].real
+        tol = 1e-6 * max(1.0, abs(x))
+        assert np.min(np.abs(real - x)) < tol
+        if len(real) == 3:
+            assert abs(abs(x) - np.min(np.abs(real))) < tol
+
+
+def test_electron_number_correction_restores_ne():
+    """correct_electron_number (DMMinModule.f90:1676-1817) brings a perturbed L back to ne electrons."""
+    n, lnv, dense, S, H = _chain()
+    lnv.iter_hott_invs()
+    lnv.transpose(lnv.T, lnv.Ttran)
+    lnv.init_mcw()
+    lnv.mcw_min(lnv.p.n_L_iterations)
+    rs = np.random.default_rng(1)
+    lnv.L.v[:] += rs.normal(size=lnv.L.v.size) * 1e-3
+    lnv.symmetrise_L()
+    before, _ = lnv.lnv(dophi=True, phi=lnv.phi)
+    lnv.correct_electron_number()
+    after, _ = lnv.lnv(dophi=True, phi=lnv.phi)
+    assert abs(before - n) > 1e-4
+    assert abs(after - n) < 1e-9
