@@ -454,6 +454,13 @@ class LNV:
         return r.as_dict(), Lo, Ko
 
 
+def solve_cubic(a, b, c, guess):
+    """SolveCubic root (host computation in libcqb200.so)."""
+    x = c_double()
+    check(lib().cq_solve_cubic(c_double(a), c_double(b), c_double(c), c_double(guess), ctypes.byref(x)))
+    return x.value
+
+
 def pulay_alphas(ipulay, Aij, n, max_n):
     """DoPulay2D_nospin mixing coefficients (host computation in libcqb200.so)."""
     A = np.zeros((max_n, max_n))

@@ -156,6 +156,13 @@ int cq_pulay_alphas(int ipulay, const double* Aij, int n, int max_n, double* alp
   });
 }
 
+int cq_solve_cubic(double a, double b, double c, double guess, double* x) {
+  return guarded_call([&] {
+    CQ_CHECK(x != nullptr, CQ_ERR_ARG, "null argument");
+    *x = LNVSolver::solve_cubic(a, b, c, guess);
+  });
+}
+
 int cq_lnv_solve(cq_lnv* s, cq_lnv_result* res) {
   return guarded_call([&] {
     CQ_CHECK(s, CQ_ERR_ARG, "null argument");

@@ -80,6 +80,7 @@ class LNVSolver {
   void force_matrices(DMat& M12, DMat& M4);
   bool use_mixed = false;   // current product arithmetic of mult_dispatch
   static void do_pulay(int iPulay, const double* Aij, int n, int max_n, double* al);
+  static double solve_cubic(double a, double b, double c, double guess);
   void lnv(bool doK, bool doM3, bool dophi, bool doE, DMat* M3, DMat* phim, double* electrons, double* energy);
 
  private:
@@ -116,7 +117,6 @@ class LNVSolver {
   void init_mcw();
   void mcw_mm_nonds(DMat& RhoNew, double& energy, double& c);
   double mcw_min(int n_L_iterations);
-  static double solve_cubic(double a, double b, double c, double guess);
   void correct_electron_number();
   bool line_min_L(DMat& M3, DMat& D, DMat& mtemp, DMat& SM3, double energy_in, double& energy_out, double& zeta);
   void project_search(DMat& search, DMat& SM3, DMat& Sphi, DMat& mtemp);

@@ -289,6 +289,11 @@ int cq_lnv_put(cq_lnv* s, const char* name, const double* in, int on_device);
  * the unit vector e_ipulay.  Host-only, needs no GPU.
  */
 int cq_pulay_alphas(int ipulay, const double* Aij, int n, int max_n, double* alphas);
+/* SolveCubic (src/DMMinModule.f90:2072-2143): a real root of x^3 + a x^2 + b x + c = 0 by
+ * Cardano's formula, the one of least magnitude when there are three; with one real root farther
+ * than 10 |guess| from zero, guess.  The root the electron-number correction steps to.  Host-only,
+ * needs no GPU. */
+int cq_solve_cubic(double a, double b, double c, double guess, double* x);
 
 /* One complete solve on the device-resident S and H: T = S^-1, then FindMinDM from the McWeeny start. */
 int cq_lnv_solve(cq_lnv* s, cq_lnv_result* res);

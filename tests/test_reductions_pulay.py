@@ -70,3 +70,12 @@ def test_pulay_nan_matrix_is_singular():
     assert al[1] == 1.0 and al[0] == 0.0 and al[2] == 0.0
     assert bk_inverse([list(r) for r in A]) is None
     assert not math.isnan(al.sum())
+
+
+def test_solve_cubic_library_equals_oracle():
+    """The library's SolveCubic (host C++) and the oracle's restatement give the same bits."""
+    rs = np.random.default_rng(7)
+    for _ in range(2000):
+        a, b, c = rs.normal(size=3) * rs.choice([0.1, 1.0, 10.0], 3)
+        g = float(rs.choice([1e-3, 1.0, 1e6]))
+        assert cq_b200.solve_cubic(a, b, c, g) == OracleLNV.solve_cubic(a, b, c, g)
