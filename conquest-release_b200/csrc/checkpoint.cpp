@@ -179,6 +179,7 @@ int64_t grab_matrix_file(System& S, int r, double* dev, const std::string& path)
     for (int s = 1; s < nspin; ++s)
       for (int64_t k = 0; k < len; ++k) rd.one<double>();     // further spin channels: not used here
     const int p = g.global_to_prim[idi - 1];
+    CQ_CHECK(p >= 0, CQ_ERR_ARG, "matrix file: atom is not a primary atom of this system");
     CQ_CHECK(nsf_i[q] == g.nsf[idi - 1], CQ_ERR_ARG, "matrix file: block size of an atom differs");
     int64_t off = 0;
     for (int jj = 0; jj < jmax[q]; ++jj) {
