@@ -181,6 +181,7 @@ class System:
         # handles of the LNV solvers built on this system: close() destroys them first, whatever
         # order the garbage collector finalises the Python objects in
         self._lnvs = set()
+        self._bound = {}          # matrix id -> host array bound to it (kept alive here)
 
     @property
     def handle(self):
@@ -229,6 +230,48 @@ class System:
         """precision: PREC_FP64 (default kernel rounding), PREC_FP64_FMA, PREC_BF16X3 (tensor cores)."""
         prec = int(bool(exact)) if precision is None else int(precision)
         check(lib().cq_mat_mult(self._h, mult_type, ra, rb, rc, _ptr(a), _ptr(b), _ptr(c), prec))
+
+    # ---- matrices by id (cq_matrix_*: the device side of mat_p(id)%matrix) ----------------
+    def bind(self, mid, r, host=None):
+        """Bind matrix id `mid` to range r: a zeroed device copy owned by the system.  `host` (a
+        contiguous float64 array of the range's length, referenced here) is what upload() and
+        download() copy from and to."""
+        if host is not None and not (isinstance(host, np.ndarray) and host.dtype == np.float64
+                                     and host.flags.c_contiguous and host.size == self.length(r)):
+            raise ValueError("host must be a contiguous float64 array of the range's length")
+        check(lib().cq_matrix_bind(self._h, int(mid), int(r), _dp(host) if host is not None else None))
+        self._bound[int(mid)] = host
+
+    def unbind(self, mid):
+        check(lib().cq_matrix_unbind(self._h, int(mid)))
+        self._bound.pop(int(mid), None)
+
+    def upload(self, mid):
+        check(lib().cq_matrix_upload(self._h, int(mid)))
+
+    def download(self, mid):
+        """Copy the device copy into the bound host array (synchronising) and return that array."""
+        check(lib().cq_matrix_download(self._h, int(mid)))
+        return self._bound[int(mid)]
+
+    def device_ptr(self, mid):
+        p, n = c_void_p(), c_int64()
+        check(lib().cq_matrix_device(self._h, int(mid), ctypes.byref(p), ctypes.byref(n)))
+        return p.value, n.value
+
+    def product_id(self, mult_type, ida, idb, idc, precision=PREC_FP64):
+        check(lib().cq_matrix_product_id(self._h, int(mult_type), int(ida), int(idb), int(idc), int(precision)))
+
+    def sum_id(self, ida, alpha, idb, beta):
+        check(lib().cq_matrix_sum_id(self._h, int(ida), c_double(alpha), int(idb), c_double(beta)))
+
+    def transpose_id(self, ida, idat):
+        check(lib().cq_matrix_transpose_id(self._h, int(ida), int(idat)))
+
+    def product_trace_id(self, ida, idb):
+        v = c_double()
+        check(lib().cq_matrix_product_trace_id(self._h, int(ida), int(idb), ctypes.byref(v)))
+        return v.value
 
     def mat_mult_host(self, mult_type, ra, rb, rc, a, b, c, exact=True, precision=None):
         for arr in (a, b, c):

@@ -81,10 +81,20 @@ void launch_dropin(int type, const int64_t* d_out, const int* d_dims, const int6
 
 using namespace cqb;
 
+// A matrix bound to an id (cq_matrix_bind): the system-owned device copy in the layout of its
+// range, and the caller's host array it is copied from and to on demand.
+struct BoundMatrix {
+  int r = -1;
+  double* host = nullptr;
+  DevBuf<double> dev;
+};
+
 struct cq_system {
   cqb::System S;
   // staging buffers of the host-memory entry points
   DevBuf<double> ha, hb, hc;
+  // matrices by id; destroyed before S, whose stream their memory is released on
+  std::map<int, std::unique_ptr<BoundMatrix>> store;
 };
 
 template <class F>
@@ -454,6 +464,114 @@ int cq_m_kern_min(int k_off, int kpart, const int* ib_nd_acc, const int* ibaddr,
   return dropin(2, k_off, kpart, ib_nd_acc, ibaddr, nbnab, ibpart, ibseq, bndim2, a, b, const_cast<double*>(c),
                 ahalo_nh_part, ahalo_j_beg, ahalo_j_seq, ahalo_ndimi, ahalo_ndimj, chalo_i_halo, chalo_i_hbeg,
                 chalo_i_h2d, chalo_ni_in_halo, at_i_prim, at_i_beg, at_i_nd_beg, at_n_hnab, lena, lenb, lenc);
+}
+
+// ---- matrices by id (the device side of mat_p(id)%matrix) ----------------------------------
+static BoundMatrix& bound(cq_system* sys, int id) {
+  auto it = sys->store.find(id);
+  CQ_CHECK(it != sys->store.end(), CQ_ERR_ARG, "matrix id " + std::to_string(id) + " is not bound");
+  return *it->second;
+}
+
+int cq_matrix_bind(cq_system* sys, int id, int r, double* host) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, r);
+    CQ_CHECK(sys->store.find(id) == sys->store.end(), CQ_ERR_STATE,
+             "matrix id " + std::to_string(id) + " is already bound");
+    auto m = std::make_unique<BoundMatrix>();
+    const int64_t n = std::max<int64_t>(sys->S.ranges[r]->length, 1);
+    m->r = r;
+    m->host = host;
+    m->dev.alloc((size_t)n, sys->S.stream);
+    CQ_CUDA(cudaMemsetAsync(m->dev.p, 0, sizeof(double) * n, sys->S.stream));
+    sys->store[id] = std::move(m);
+  });
+}
+
+int cq_matrix_unbind(cq_system* sys, int id) {
+  return guarded([&] {
+    check_sys(sys);
+    bound(sys, id);
+    sys->store.erase(id);
+  });
+}
+
+int cq_matrix_device(cq_system* sys, int id, double** dev, int64_t* length) {
+  return guarded([&] {
+    check_sys(sys);
+    BoundMatrix& m = bound(sys, id);
+    if (dev) *dev = m.dev.p;
+    if (length) *length = sys->S.ranges[m.r]->length;
+  });
+}
+
+int cq_matrix_upload(cq_system* sys, int id) {
+  return guarded([&] {
+    check_sys(sys);
+    BoundMatrix& m = bound(sys, id);
+    CQ_CHECK(m.host != nullptr, CQ_ERR_STATE, "matrix id " + std::to_string(id) + " has no host array");
+    const int64_t n = sys->S.ranges[m.r]->length;
+    if (n) CQ_CUDA(cudaMemcpyAsync(m.dev.p, m.host, sizeof(double) * n, cudaMemcpyHostToDevice, sys->S.stream));
+  });
+}
+
+int cq_matrix_download(cq_system* sys, int id) {
+  return guarded([&] {
+    check_sys(sys);
+    BoundMatrix& m = bound(sys, id);
+    CQ_CHECK(m.host != nullptr, CQ_ERR_STATE, "matrix id " + std::to_string(id) + " has no host array");
+    const int64_t n = sys->S.ranges[m.r]->length;
+    if (n) CQ_CUDA(cudaMemcpyAsync(m.host, m.dev.p, sizeof(double) * n, cudaMemcpyDeviceToHost, sys->S.stream));
+    CQ_CUDA(cudaStreamSynchronize(sys->S.stream));
+  });
+}
+
+int cq_matrix_product_id(cq_system* sys, int mult_type, int ida, int idb, int idc, int precision) {
+  return guarded([&] {
+    check_sys(sys);
+    CQ_CHECK(mult_type == 1 || mult_type == 2, CQ_ERR_ARG, "mult_type must be 1 or 2");
+    CQ_CHECK(precision == CQ_PREC_FP64 || precision == CQ_PREC_FP64_FMA || precision == CQ_PREC_BF16X3, CQ_ERR_ARG,
+             "unknown precision");
+    const int out = mult_type == 1 ? idc : ida;
+    CQ_CHECK(out != (mult_type == 1 ? ida : idc) && out != idb, CQ_ERR_ARG, "the product's output must not be an input");
+    BoundMatrix &A = bound(sys, ida), &B = bound(sys, idb), &C = bound(sys, idc);
+    ProductPlan& P = get_plan(sys->S, mult_type, A.r, B.r, C.r);
+    if (precision == CQ_PREC_BF16X3) mat_mult_mixed(sys->S, mult_type, A.r, B.r, C.r, A.dev.p, B.dev.p, C.dev.p);
+    else launch_mat_mult(sys->S, P, A.dev.p, B.dev.p, C.dev.p, precision);
+  });
+}
+
+int cq_matrix_sum_id(cq_system* sys, int ida, double alpha, int idb, double beta) {
+  return guarded([&] {
+    check_sys(sys);
+    BoundMatrix &A = bound(sys, ida), &B = bound(sys, idb);
+    System& S = sys->S;
+    if (A.r == B.r) {
+      dev_scale(S, A.dev.p, S.ranges[A.r]->length, alpha);
+      dev_axpy(S, A.dev.p, S.ranges[A.r]->length, beta, B.dev.p);
+    } else {
+      dev_matrix_add(S, A.r, A.dev.p, alpha, B.r, B.dev.p, beta);
+    }
+  });
+}
+
+int cq_matrix_transpose_id(cq_system* sys, int ida, int idat) {
+  return guarded([&] {
+    check_sys(sys);
+    BoundMatrix &A = bound(sys, ida), &AT = bound(sys, idat);
+    CQ_CHECK(A.r == AT.r && ida != idat, CQ_ERR_ARG, "transpose: two different matrices of one range");
+    dev_transpose(sys->S, A.r, A.dev.p, AT.dev.p);
+  });
+}
+
+int cq_matrix_product_trace_id(cq_system* sys, int ida, int idb, double* result) {
+  return guarded([&] {
+    check_sys(sys);
+    CQ_CHECK(result != nullptr, CQ_ERR_ARG, "null result");
+    BoundMatrix &A = bound(sys, ida), &B = bound(sys, idb);
+    CQ_CHECK(A.r == B.r, CQ_ERR_ARG, "product trace: both matrices of one range");
+    *result = dev_dot(sys->S, A.dev.p, B.dev.p, sys->S.ranges[A.r]->length);
+  });
 }
 
 }  // extern "C"

@@ -115,6 +115,33 @@ int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, doub
                      int precision);
 
 /*
+ * Matrices by id: the HBM side of mat_p(id)%matrix (src/matrix_data_module.f90).  The system owns
+ * one device copy per bound id, in the block layout of the id's range; the caller's host array
+ * (mat_p(id)%matrix) is copied on demand.  The operations mirror mult_module's by-index calls
+ * (matrix_product, matrix_sum, matrix_transpose, matrix_product_trace; src/mult_module.f90:
+ * 2556-2916) on those device copies, enqueued on the system's stream.
+ *   cq_matrix_bind      allocate the zeroed device copy of id in range r; host (range length
+ *                       doubles, may be NULL) is remembered, not copied; an id binds once
+ *   cq_matrix_unbind    release it
+ *   cq_matrix_device    its device pointer and length (for cq_mat_mult and the other entries)
+ *   cq_matrix_upload    host -> device (stream-ordered); cq_matrix_download device -> host
+ *                       (synchronises)
+ *   cq_matrix_product_id  mult_type 1: idc = ida . idb; 2: ida = idc . idb^T (ranges from the
+ *                       bound ids; the output must not be an input)
+ *   cq_matrix_sum_id    ida = alpha ida + beta idb (any two ranges, as matrix_sum)
+ *   cq_matrix_transpose_id / cq_matrix_product_trace_id  as cq_matrix_transpose / _product_trace
+ */
+int cq_matrix_bind(cq_system* sys, int id, int r, double* host);
+int cq_matrix_unbind(cq_system* sys, int id);
+int cq_matrix_device(cq_system* sys, int id, double** dev, int64_t* length);
+int cq_matrix_upload(cq_system* sys, int id);
+int cq_matrix_download(cq_system* sys, int id);
+int cq_matrix_product_id(cq_system* sys, int mult_type, int ida, int idb, int idc, int precision);
+int cq_matrix_sum_id(cq_system* sys, int ida, double alpha, int idb, double beta);
+int cq_matrix_transpose_id(cq_system* sys, int ida, int idat);
+int cq_matrix_product_trace_id(cq_system* sys, int ida, int idb, double* result);
+
+/*
  * Matrix files in the reference's binary format (dump_matrix2 / grab_matrix2,
  * src/store_matrix_module.f90:340-430, 1199-1421: Fortran unformatted sequential records; one
  * file per process, here one): the device array a_dev of range r is written with its block

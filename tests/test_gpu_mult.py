@@ -206,3 +206,53 @@ def test_algebra_matches_oracle(cfg2):
     assert abs(g.trace(idx["L"], tL) - o.trace(idx["L"], L)) < 1e-12 * abs(o.trace(idx["L"], L)) + 1e-14
     dot_ref = float(np.dot(L, L))
     assert abs(g.product_trace(idx["L"], tL, tL) - dot_ref) < 1e-12 * dot_ref
+
+
+def test_matrices_by_id_match_oracle(cfg2):
+    """Matrices by id (cq_matrix_*): host arrays bound to ids, uploaded, multiplied (both mult
+    types), summed (same and different ranges), transposed and traced on the system-owned device
+    copies, downloaded; bit for bit against the oracle and the pointer-based entries."""
+    o, g, bls, idx = cfg2
+    g.set_mult_variant(-1)
+    L = inputs.random_blocks(bls["L"], 51, inputs.TAG_RANDOM_A)
+    S = inputs.random_blocks(bls["S"], 51, inputs.TAG_RANDOM_B)
+    T = inputs.random_blocks(bls["T"], 52, inputs.TAG_RANDOM_B)
+    TS = inputs.random_blocks(bls["TS"], 52, inputs.TAG_RANDOM_A)
+    hL, hS, hLS = L.copy(), S.copy(), np.full(bls["LS"].length, np.nan)
+    hT, hTS, hTo = T.copy(), TS.copy(), np.full(bls["T"].length, np.nan)
+    hL2 = np.full(bls["L"].length, np.nan)
+    for mid, r, h in ((1, "L", hL), (2, "S", hS), (3, "LS", hLS), (4, "T", hT), (5, "TS", hTS), (6, "T", hTo),
+                      (7, "L", hL2)):
+        g.bind(mid, idx[r], h)
+    for mid in (1, 2, 4, 5):
+        g.upload(mid)
+    # type 1: LS = L . S
+    g.product_id(1, 1, 2, 3)
+    ref = np.zeros(bls["LS"].length); o.mat_mult(1, idx["L"], idx["S"], idx["LS"], L, S, ref)
+    assert np.array_equal(g.download(3), ref)
+    # type 2: T_out = TS . T^T
+    g.product_id(2, 6, 4, 5)
+    ref2 = np.zeros(bls["T"].length); o.mat_mult(2, idx["T"], idx["T"], idx["TS"], ref2, T, TS)
+    assert np.array_equal(g.download(6), ref2)
+    # transpose into a second L-range matrix, then sums of equal and of different ranges
+    g.transpose_id(1, 7)
+    assert np.array_equal(g.download(7), o.transpose(idx["L"], L))
+    g.sum_id(7, 0.5, 1, -2.0)
+    ref3 = o.transpose(idx["L"], L) * 0.5 + (-2.0 * L)
+    assert np.array_equal(g.download(7), ref3)
+    g.sum_id(2, 0.0, 3, 3.0)
+    ref4 = S.copy(); o.matrix_add(0.0, ref4, idx["S"], 3.0, ref, idx["LS"])
+    assert np.array_equal(g.download(2), ref4)
+    # product trace by id equals the pointer-based entry on the same device arrays
+    p1, n1 = g.device_ptr(1)
+    p7, _ = g.device_ptr(7)
+    assert n1 == bls["L"].length
+    assert g.product_trace_id(1, 7) == g.product_trace(idx["L"], p1, p7)
+    # an id binds once; unbound ids are rejected
+    import cq_b200
+    with pytest.raises(cq_b200.CQError):
+        g.bind(1, idx["L"], hL)
+    for mid in range(1, 8):
+        g.unbind(mid)
+    with pytest.raises(cq_b200.CQError):
+        g.upload(1)
