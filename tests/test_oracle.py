@@ -166,3 +166,28 @@ def test_trace_is_onsite_diagonal(sz_small):
             blk = a[bl.elem_off[q]:bl.elem_off[q] + 16].reshape(4, 4)
             tr += np.trace(blk)
     assert abs(o.trace(1, a) - tr) < 1e-12
+
+
+@pytest.mark.parametrize("case", ["one_atom", "two_atoms_mixed_sizes"])
+def test_tiny_cells_match_image_arithmetic(case):
+    """Edge cases: a one-atom cell whose neighbours are all its own periodic images, and a
+    two-atom cell with 4x4 and 13x13 blocks in an orthorhombic box; both mult types against
+    explicit image arithmetic."""
+    if case == "one_atom":
+        coords, cell, nsf = np.array([[0.3, 0.2, 0.1]]), np.array([5.0, 5.0, 5.0]), [4]
+    else:
+        coords, cell, nsf = np.array([[0.0, 0.0, 0.0], [2.5, 2.5, 2.5]]), np.array([5.0, 6.0, 7.0]), [4, 13]
+    o = OracleSystem(coords, cell, np.array(nsf), [4.0, 6.0, 10.0])
+    bls = [bm.oracle_blocklist(o, r, coords, cell) for r in range(3)]
+    assert len(bls[0].ig_i) == len(coords)           # range 4 < every image distance: onsite only
+    a = inputs.random_blocks(bls[0], 7, inputs.TAG_RANDOM_A)
+    b = inputs.random_blocks(bls[1], 7, inputs.TAG_RANDOM_B)
+    c = np.zeros(bls[2].length)
+    o.mat_mult(1, 0, 1, 2, a, b, c)
+    ck = bm.kat_type1(bls[0], a, bls[1], b, bls[2])
+    assert np.abs(c - ck).max() < 1e-13 * np.abs(ck).max()
+    cin = inputs.random_blocks(bls[2], 8, inputs.TAG_RANDOM_A)
+    out = np.zeros(bls[0].length)
+    o.mat_mult(2, 0, 1, 2, out, b, cin)
+    ck2 = bm.kat_type2(bls[0], bls[1], b, bls[2], cin)
+    assert np.abs(out - ck2).max() < 1e-13 * np.abs(ck2).max()
