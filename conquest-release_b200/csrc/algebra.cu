@@ -10,7 +10,6 @@
 // from run to run.
 #include <climits>
 #include <functional>
-#include <mutex>
 #include <cmath>
 #include <limits>
 
@@ -441,22 +440,14 @@ constexpr int kNoAllocSums = CQ_NOALLOC_MAX_SUMS;
 constexpr int kNoAllocWords = 3 * kRedBlocks + 4 * kNoAllocSums + kNoAllocSums;
 static __device__ __align__(256) uint64_t g_noalloc_scratch[kNoAllocWords];   // 28.7 KiB per device
 
-std::mutex g_noalloc_mu;
-uint64_t* g_noalloc_addr[64] = {};   // device address of g_noalloc_scratch, per device ordinal
-
-// Device address of the static scratch on the current device, looked up once per device (the
-// host-side name of the array is not a device address).
+// Device address of the static scratch on the current device.  The host-side name of the array
+// is not a device address, so it is looked up with cudaGetSymbolAddress on every call (cheap, and
+// it allocates nothing): a cached address would go stale if the host tore the context down
+// (cudaDeviceReset) between calls.
 uint64_t* noalloc_scratch() {
-  int dev = 0;
-  CQ_CUDA(cudaGetDevice(&dev));
-  CQ_CHECK(dev >= 0 && dev < 64, CQ_ERR_ARG, "device ordinal out of range");
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    CQ_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_noalloc_addr[dev] = static_cast<uint64_t*>(p);
-  }
-  return g_noalloc_addr[dev];
+  void* p = nullptr;
+  CQ_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+  return static_cast<uint64_t*>(p);
 }
 }  // namespace
 

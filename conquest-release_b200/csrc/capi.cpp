@@ -491,7 +491,11 @@ int cq_matrix_bind(cq_system* sys, int id, int r, double* host) {
 int cq_matrix_unbind(cq_system* sys, int id) {
   return guarded([&] {
     check_sys(sys);
-    bound(sys, id);
+    BoundMatrix& m = bound(sys, id);
+    // release on the stream the system uses now: the buffer may have been allocated on a stream
+    // replaced since by cq_system_set_stream (whose earlier work that call waited for), while
+    // work enqueued on the current stream may still read or write it
+    m.dev.st = sys->S.stream;
     sys->store.erase(id);
   });
 }

@@ -122,10 +122,12 @@ int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, doub
  * 2556-2916) on those device copies, enqueued on the system's stream.
  *   cq_matrix_bind      allocate the zeroed device copy of id in range r; host (range length
  *                       doubles, may be NULL) is remembered, not copied; an id binds once
- *   cq_matrix_unbind    release it
+ *   cq_matrix_unbind    release it (on the system's current stream, after the work enqueued there)
  *   cq_matrix_device    its device pointer and length (for cq_mat_mult and the other entries)
- *   cq_matrix_upload    host -> device (stream-ordered); cq_matrix_download device -> host
- *                       (synchronises)
+ *   cq_matrix_upload    host -> device, stream-ordered: the call returns once the copy is queued,
+ *                       so the host array must stay unchanged (and allocated) until the next call
+ *                       on the system that synchronises (cq_matrix_download, cq_synchronize);
+ *                       cq_matrix_download device -> host (synchronises)
  *   cq_matrix_product_id  mult_type 1: idc = ida . idb; 2: ida = idc . idb^T (ranges from the
  *                       bound ids; the output must not be an input)
  *   cq_matrix_sum_id    ida = alpha ida + beta idb (any two ranges, as matrix_sum)
@@ -342,8 +344,9 @@ int cq_lnv_solve_host(cq_lnv* s, const double* S, const double* H, double* L_out
  * `stream` (a cudaStream_t, NULL = the default stream) and the call synchronises it.
  *   - At most CQ_NOALLOC_MAX_SUMS sums per call; more is rejected with CQ_ERR_ARG.
  *   - The scratch is one static device array of 28.7 KiB that every GPU loading the library
- *     holds until exit.  The first call on each device looks up that array's device address;
- *     make it before any stream capture on that device.
+ *     holds until exit.  Every call looks up that array's device address on the current device
+ *     (the first lookup on a device may load the library's device code there: make the first
+ *     call before any stream capture on that device).
  *   - Every call shares the array: calls that overlap on the GPU (two streams, two threads) race
  *     and give wrong sums.  Serialise them.
  */

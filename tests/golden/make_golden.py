@@ -13,7 +13,11 @@ lnv_scf_si64.json holds the same quantities for the chain with mixed-L self-cons
 after every Pulay step, a linear density feedback standing in for the grid rebuild of H, plus the
 number of rebuilds and a SHA-256 of the final H.
 
-    python tests/golden/make_golden.py [chain|scf]      (default: both)
+lnv_chain_si512.json holds the same quantities for the benchmark workload: the 512-atom Si supercell
+(4x4x4 cells, sigma 0.1 bohr, seed 2), SZ blocks, S/H/L/T ranges 10/12/16/10 bohr, 1024 electrons,
+50 LNV iterations, tolerance 1e-7, solved to convergence.  It takes several minutes on the CPU.
+
+    python tests/golden/make_golden.py [chain|scf|bench]      (default: chain and scf)
 """
 import hashlib
 import json
@@ -35,13 +39,13 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 CASES = {"r8_9_10_8": ((8.0, 9.0, 10.0, 8.0), 2), "r10_12_16_10": ((10.0, 12.0, 16.0, 10.0), 40)}
 
 
-def run_case(ranges, max_outer, feedback=None):
+def run_case(ranges, max_outer, feedback=None, ncell=2):
     import blockmaps as bm
     import cq_b200
     from cq_b200 import inputs
     from cq_oracle import OracleSystem
     from lnv_oracle import OracleLNV, Params
-    coords, cell = inputs.diamond_si(2, sigma=0.1, seed=2)
+    coords, cell = inputs.diamond_si(ncell, sigma=0.1, seed=2)
     n = len(coords)
     rng = cq_b200.lnv_ranges(*ranges)
     ridx = {k: i for i, k in enumerate(rng)}
@@ -69,6 +73,14 @@ SCF_CASES = {"r8_9_10_8_gm005": ((8.0, 9.0, 10.0, 8.0), 1, -0.05)}
 
 
 def main(which=("chain", "scf")):
+    if "bench" in which:
+        out = {"system": "diamond Si 4x4x4 cells (512 atoms), sigma 0.1 bohr, seed 2; S overlap_S, H hamiltonian_H "
+                         "seed 5; 4x4 blocks; ne_spin = 512 (1024 electrons); the benchmark workload", "cases": {}}
+        t = time.time()
+        out["cases"]["r10_12_16_10"] = run_case((10.0, 12.0, 16.0, 10.0), 40, ncell=4)
+        out["cases"]["r10_12_16_10"]["oracle_seconds"] = round(time.time() - t, 1)
+        print("si512", out["cases"]["r10_12_16_10"]["energy"], "%.1f s" % (time.time() - t), flush=True)
+        json.dump(out, open(os.path.join(HERE, "lnv_chain_si512.json"), "w"), indent=1)
     if "scf" in which:
         out = {"system": "diamond Si 2x2x2 cells (64 atoms), sigma 0.1 bohr, seed 2; S overlap_S, H0 hamiltonian_H "
                          "seed 5; 4x4 blocks; ne_spin = 64; H = H0 + g K rebuilt by lateDM", "cases": {}}

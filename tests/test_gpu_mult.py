@@ -256,3 +256,37 @@ def test_matrices_by_id_match_oracle(cfg2):
         g.unbind(mid)
     with pytest.raises(cq_b200.CQError):
         g.upload(1)
+
+
+def test_unbind_after_stream_switch_keeps_inflight_inputs(cfg2):
+    """Matrices bound on the system's own stream, then a switch to a torch stream: a product by id is
+    enqueued there, its inputs are unbound while it may still run, and new ids bound and filled
+    at once (allocations that may reuse the released memory).  The release happens on the current
+    stream, after the product, so the product still reads its own inputs: bit for bit against the
+    oracle."""
+    import torch
+    o, g, bls, idx = cfg2
+    g.set_mult_variant(-1)
+    L = inputs.random_blocks(bls["L"], 61, inputs.TAG_RANDOM_A)
+    S = inputs.random_blocks(bls["S"], 61, inputs.TAG_RANDOM_B)
+    hL, hS, hLS = L.copy(), S.copy(), np.full(bls["LS"].length, np.nan)
+    g.bind(11, idx["L"], hL); g.bind(12, idx["S"], hS); g.bind(13, idx["LS"], hLS)
+    g.upload(11); g.upload(12)
+    g.synchronize()
+    st = torch.cuda.Stream()
+    g.set_stream(st.cuda_stream)
+    try:
+        junkL, junkS = np.full(bls["L"].length, 7.0), np.full(bls["S"].length, -3.0)
+        for _ in range(3):
+            g.product_id(1, 11, 12, 13)
+        g.unbind(11); g.unbind(12)
+        g.bind(14, idx["L"], junkL); g.bind(15, idx["S"], junkS)
+        g.upload(14); g.upload(15)
+        ref = np.zeros(bls["LS"].length)
+        o.mat_mult(1, idx["L"], idx["S"], idx["LS"], L, S, ref)
+        assert np.array_equal(g.download(13), ref)
+        for mid in (13, 14, 15):
+            g.unbind(mid)
+        g.synchronize()
+    finally:
+        g.set_stream(None)
