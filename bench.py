@@ -33,6 +33,7 @@ sys.path.insert(0, os.path.join(ROOT, "conquest-release_b200"))
 METRIC = "LNV solves/s (FP64, 512-atom Si SZ)"
 WORKLOAD = "lnv512_si_sz_fp64"
 CFG = dict(ncell=4, sigma=0.1, seed=2, rs=10.0, rh=12.0, rl=16.0, rt=10.0, nsf=4, ne_per_atom=2.0, h_seed=5)
+SAMPLE_S = 5.0     # seconds of CPU chain per timed sample (reference arm step, cpu_baseline leg)
 
 
 def build_problem(cq_b200):
@@ -156,25 +157,64 @@ def lnv_call_products():
             (2, "H", "LS", "LSL")]
 
 
-def cpu_lnv_call(prob, nthreads):
-    """Time one LNV_matrix_multiply(M3, phi, E) call of the oracle's ompGemm chain on the host cores."""
+class _SampleDone(Exception):
+    pass
+
+
+def cpu_chain_setup(coords, cell, ridx, S, H, ne_spin, nthreads):
+    """The oracle's restatement of the chain with the ompGemm kernel on `nthreads` host threads, set up to the
+    point where FindMinDM's iterations start: T = S^-1 (Hotelling) and the McWeeny initial L (untimed).
+    Returns (chain, L after the McWeeny start, its energy change)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    os.environ["OMP_NUM_THREADS"] = str(nthreads)
     from cq_oracle import OracleSystem
     from lnv_oracle import OracleLNV, Params
-    os.environ["OMP_NUM_THREADS"] = str(nthreads)
     import cq_b200
     rng = cq_b200.lnv_ranges(CFG["rs"], CFG["rh"], CFG["rl"], CFG["rt"])
-    o = OracleSystem(prob["coords"], prob["cell"], np.full(prob["n"], CFG["nsf"]), list(rng.values()))
-    lnv = OracleLNV(o, prob["ridx"], prob["S"], prob["H"], prob["ne_spin"], float(CFG["nsf"] * prob["n"]), Params(),
-                    kernel="ompGemm", nthreads=nthreads)
-    rs = np.random.default_rng(0)
-    lnv.L.v[:] = rs.uniform(-0.01, 0.01, size=lnv.L.v.size)
-    M3 = lnv.temp("L")
-    import cq_oracle
-    cq_oracle._load()
+    n = len(coords)
+    o = OracleSystem(coords, cell, np.full(n, CFG["nsf"]), list(rng.values()))
+    lnv = OracleLNV(o, ridx, S, H, ne_spin, float(CFG["nsf"] * n), Params(), kernel="ompGemm", nthreads=nthreads)
+    lnv.iter_hott_invs()
+    lnv.transpose(lnv.T, lnv.Ttran)
+    lnv.init_mcw()
+    de = lnv.mcw_min(lnv.p.n_L_iterations)
+    return lnv, lnv.L.v.copy(), de
+
+
+def cpu_chain_sample(lnv, L0, de0, budget_s):
+    """One timed sample of the CPU chain: FindMinDM iterations (early and late DM, line searches, electron
+    number corrections, Pulay steps: every product, sum, transpose and trace of the chain) from the McWeeny
+    start, stopped before the first product that begins after `budget_s` seconds.
+    Returns (seconds, algorithmic flops of the products run, products run)."""
+    lnv.L.v[:] = L0
+    lnv.delta_e = de0
+    f0, p0 = lnv.flops, lnv.n_products
     t0 = time.perf_counter()
-    lnv.lnv(doM3=True, dophi=True, doE=True, M3=M3, phi=lnv.phi)
-    return time.perf_counter() - t0
+
+    def stop(_):
+        if time.perf_counter() - t0 > budget_s:
+            raise _SampleDone()
+    lnv.before_product = stop
+    try:
+        lnv.find_min_dm(resetL=False)
+    except _SampleDone:
+        pass
+    finally:
+        lnv.before_product = None
+    return time.perf_counter() - t0, lnv.flops - f0, lnv.n_products - p0
+
+
+def cpu_record():
+    """The committed record of one complete CPU solve of the workload timed on the GPU box's host cores
+    (profiles/cpu_solve_lnv512.json), or None."""
+    p = os.path.join(ROOT, "profiles", "cpu_solve_lnv512.json")
+    return json.load(open(p)) if os.path.exists(p) else None
+
+
+def config_of(n, ne_spin, ws):
+    return {"workload": WORKLOAD, "atoms": n, "blocks": "4x4", "ranges_bohr": {"S": 10, "H": 12, "L": 16, "T": 10},
+            "electrons": int(2 * ne_spin), "n_L_iterations": 50, "tolerance": 1e-7,
+            "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas x%d" % ws}
 
 
 def flops_of_lnv_call(system, ridx):
@@ -212,19 +252,21 @@ def emit(line):
 
 
 def reference_main(args, ws, rank):
-    """CPU arm: the oracle's restatement of the reference's ompGemm chain on all host cores (rank 0 only).
+    """CPU arm: the oracle's restatement of the reference's chain with the ompGemm kernel (OpenMP over all host
+    cores, OpenBLAS dgemm with one thread), rank 0 only.
 
-    Each step is one LNV_matrix_multiply(M3, phi, E) call on the workload (a bounded sample of a solve);
-    solves/s = measured flop rate / flops of one solve, with the solve's flop count and the call's flop count
-    taken from the committed work record of the workload (profiles/lnv512_solve_work.json).
+    Set-up (untimed, once): geometry, indices, S, H, T = S^-1 and the McWeeny start.  Each step then times a
+    bounded sample of the solve, FindMinDM's iterations from the McWeeny start for about SAMPLE_S seconds, and
+    counts the algorithmic flops of the products it ran.  solves/s = that flop rate / the flops of one complete
+    solve (counted from the same chain's products, profiles/lnv512_solve_work.json).  A complete CPU solve timed
+    once on the same host is reported beside it (profiles/cpu_solve_lnv512.json).
     """
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from cq_b200 import inputs
-    from cq_oracle import OracleSystem
-    from lnv_oracle import OracleLNV, Params
     import cq_b200
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from cq_oracle import OracleSystem
     rec = json.load(open(work_record_path()))
     coords, cell = inputs.diamond_si(CFG["ncell"], sigma=CFG["sigma"], seed=CFG["seed"])
     n = len(coords)
@@ -233,29 +275,32 @@ def reference_main(args, ws, rank):
     o = OracleSystem(coords, cell, np.full(n, CFG["nsf"]), list(rng.values()))
     S = inputs.overlap_S(o.blocklist(ridx["S"], coords, cell))
     H = inputs.hamiltonian_H(o.blocklist(ridx["H"], coords, cell), seed=CFG["h_seed"])
+    ne_spin = CFG["ne_per_atom"] * n / 2.0
     nth = os.cpu_count() or 1
-    lnv = OracleLNV(o, ridx, S, H, CFG["ne_per_atom"] * n / 2.0, float(CFG["nsf"] * n), Params(), kernel="ompGemm",
-                    nthreads=nth)
-    lnv.L.v[:] = np.random.default_rng(0).uniform(-0.01, 0.01, size=lnv.L.v.size)
-    M3 = lnv.temp("L")
-    for _ in range(args.warmup if args.warmup <= 1 else 1):
-        lnv.lnv(doM3=True, dophi=True, doE=True, M3=M3, phi=lnv.phi)
-    times = []
+    lnv, L0, de0 = cpu_chain_setup(coords, cell, ridx, S, H, ne_spin, nth)
+    for _ in range(min(args.warmup, 1)):
+        cpu_chain_sample(lnv, L0, de0, 1.0)
+    secs, flops, prods = [], [], []
     for _ in range(args.steps):
-        t0 = time.perf_counter()
-        lnv.lnv(doM3=True, dophi=True, doE=True, M3=M3, phi=lnv.phi)
-        times.append(time.perf_counter() - t0)
-    t = float(np.median(times))
-    value = rec["flops_per_lnv_call"] / t / rec["flops_per_solve"]
-    sample = ("one LNV_matrix_multiply(M3, phi, E) call (9 products, %.3g flop) of the ompGemm restatement per step, "
-              "median %.2f s on %d threads, extrapolated to one solve's %.3g flop" %
-              (rec["flops_per_lnv_call"], t, nth, rec["flops_per_solve"]))
-    emit({"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
-          "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-          "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Si supercell, S/H generators)",
-          "config": {"workload": WORKLOAD, "atoms": n, "blocks": "4x4"},
-          "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nth, "kind": "port", "sample": sample},
-          "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        t, f, pr = cpu_chain_sample(lnv, L0, de0, SAMPLE_S)
+        secs.append(t); flops.append(f); prods.append(pr)
+    rate = sum(flops) / sum(secs)                     # flop/s of the chain on the host cores
+    solve_s = rec["flops_per_solve"] / rate           # seconds per solve at that rate
+    value = 1.0 / solve_s
+    full = cpu_record()
+    sample = ("timed: FindMinDM iterations of the workload from its McWeeny start (T = S^-1 and the start set up "
+              "once, untimed), about %.0f s per step, %d steps: %d products, %.3g flop in %.1f s on %d threads "
+              "(%.3g flop/s); one solve = %.3g flop of products -> %.0f s per solve" %
+              (SAMPLE_S, args.steps, sum(prods), sum(flops), sum(secs), nth, rate, rec["flops_per_solve"], solve_s))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": solve_s * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Si supercell, S/H generators)",
+            "config": config_of(n, ne_spin, ws),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nth, "kind": "port", "sample": sample,
+                             "sample_ms_per_step": 1e3 * float(np.mean(secs)),
+                             "full_solve_timed": full},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    emit(line)
 
 
 def main():
@@ -271,6 +316,9 @@ def main():
                          "block products (216-atom DZP C=A.B; the products of one 512-atom LNV call)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3"])
     ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (-1 autotuned, 0..3, 5)")
+    ap.add_argument("--mixed-kernel", type=int, default=-1, choices=[-1, 0, 1],
+                    help="split-precision products: -1 = the faster, timed per product (default), 0 = tcgen05 tiles, "
+                         "1 = one block per mma.sync warp")
     ap.add_argument("--work-record", default=None,
                     help="write the workload's per-solve work (flops, products, energy) as JSON to this path")
     ap.add_argument("--one-solve", action="store_true",
@@ -391,21 +439,22 @@ def main():
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
             nth = os.cpu_count() or 1
-            t_cpu = cpu_lnv_call(prob, nth)
-            cpu_rate = fl_call / t_cpu
-            cpu = {"value": cpu_rate / per_solve_flops, "unit": "solves/s", "cores": nth, "kind": "port",
-                   "sample": "one LNV_matrix_multiply(M3, phi, E) call (9 products, %.3g flop) of the ompGemm "
-                             "restatement in %.2f s on %d threads, extrapolated to the solve's %.3g flop" %
-                             (fl_call, t_cpu, nth, per_solve_flops)}
+            lnv_c, L0, de0 = cpu_chain_setup(prob["coords"], prob["cell"], prob["ridx"], prob["S"], prob["H"],
+                                             prob["ne_spin"], nth)
+            t_c, f_c, p_c = cpu_chain_sample(lnv_c, L0, de0, 2 * SAMPLE_S)
+            rate_c = f_c / t_c
+            cpu = {"value": rate_c / per_solve_flops, "unit": "solves/s", "cores": nth, "kind": "port",
+                   "sample": "timed: FindMinDM iterations of this solve on the oracle's ompGemm chain from the McWeeny "
+                             "start (set up untimed): %d products, %.3g flop in %.1f s on %d threads; one solve = "
+                             "%.3g flop of products" % (p_c, f_c, t_c, nth, per_solve_flops),
+                   "full_solve_timed": cpu_record()}
         clocks = clk.summary()
         srt = sorted(steps_ms)
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Si supercell, S/H generators)",
-            "config": {"workload": WORKLOAD, "atoms": prob["n"], "blocks": "4x4", "ranges_bohr": {"S": 10, "H": 12, "L": 16, "T": 10},
-                       "electrons": int(2 * prob["ne_spin"]), "n_L_iterations": 50, "tolerance": 1e-7,
-                       "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas x%d" % ws},
+            "config": config_of(prob["n"], prob["ne_spin"], ws),
             "latency_ms": {"p50": float(np.percentile(srt, 50)), "p99": float(np.percentile(srt, 99))},
             "solve": {"energy": res["energy"], "electrons": res["electrons"], "products": res["n_products"],
                       "flops": per_solve_flops, "late_iters": res["late_iters"], "early_iters": res["early_iters"],
@@ -589,6 +638,7 @@ def mult_main(args):
     g.set_stream(stream.cuda_stream)
     if args.variant is not None:
         g.set_mult_variant(args.variant)
+    g.set_mixed_kernel(args.mixed_kernel)
     out = []
     with ClockSampler(0) as clk:
         for (name, t, ra, rb, rc, A, B, C) in prods:
@@ -608,8 +658,13 @@ def mult_main(args):
             m = float(np.median(ms))
             nbytes = 8.0 * (g.length(ra) + g.length(rb) + g.length(rc))
             tv, tms = g.product_tuning(t, ra, rb, rc, mixed=(args.precision == "bf16x3"))
+            tensor = None
+            if args.precision == "bf16x3" and args.mixed_kernel != 1:
+                nt, issued, usable = g.product_tensor_work(t, ra, rb, rc)
+                tensor = {"tiles": nt, "issued_tflop": issued / 1e12, "useful_fraction": 3.0 * flops / max(issued, 1),
+                          "issued_tflops": issued / (m / 1e3) / 1e12}
             out.append({"product": name, "triples": triples, "flops": flops, "ms": m, "tuned_variant": tv,
-                        "tune_ms": tms,
+                        "tune_ms": tms, "tensor": tensor,
                         "tflops": flops / (m / 1e3) / 1e12, "gbs_algorithmic": nbytes / (m / 1e3) / 1e9})
     tot_fl = sum(o["flops"] for o in out)
     tot_ms = sum(o["ms"] for o in out)
@@ -617,6 +672,7 @@ def mult_main(args):
           "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
           "dtype": {"fp64": "f64", "fma": "f64", "bf16x3": "bf16x3"}[args.precision],
           "data": "synthetic", "config": {"workload": args.workload, "system": desc, "variant": args.variant,
+                                          "mixed_kernel": args.mixed_kernel,
                                           "l2": "flushed (256 MB write) before every timed launch"},
           "products": out, "clocks": clk.summary()})
 

@@ -95,6 +95,7 @@ def lib():
         "cq_product_work": [c_void_p, c_int, c_int, c_int, c_int, P(c_int64), P(c_int64)],
         "cq_product_tuning": [c_void_p, c_int, c_int, c_int, c_int, P(c_int), P(ctypes.c_float), P(c_int),
                               P(ctypes.c_float)],
+        "cq_product_tensor_work": [c_void_p, c_int, c_int, c_int, c_int, P(c_int64), P(c_int64), P(c_int)],
         "cq_matrix_sum": [c_void_p, c_int, c_void_p, c_double, c_int, c_void_p, c_double],
         "cq_matrix_transpose": [c_void_p, c_int, c_void_p, c_void_p],
         "cq_matrix_trace": [c_void_p, c_int, c_void_p, P(c_double)],
@@ -293,6 +294,18 @@ class System:
         if mixed:
             return g.value, {gs: gms[i] for i, gs in enumerate((1, 2, 4, 8)) if gms[i] > 0}
         return v.value, {i: ms[i] for i in range(6) if ms[i] > 0}
+
+    def product_tensor_work(self, mult_type, ra, rb, rc):
+        """(tiles, issued tensor flops, usable) of the product's tcgen05 tile plan (cq_product_tensor_work)."""
+        t, f, u = c_int64(), c_int64(), c_int()
+        check(lib().cq_product_tensor_work(self._h, mult_type, ra, rb, rc, ctypes.byref(t), ctypes.byref(f),
+                                           ctypes.byref(u)))
+        return t.value, f.value, bool(u.value)
+
+    def set_mixed_kernel(self, k):
+        """Kernel of the split-precision products: -1 = the faster, timed per product (default), 0 = tcgen05
+        tiles, 1 = one block per mma.sync warp."""
+        check(lib().cq_system_set_option(self._h, 3, int(k)))
 
     def matrix_sum(self, ra, a, alpha, rb, b, beta):
         check(lib().cq_matrix_sum(self._h, ra, _ptr(a), float(alpha), rb, _ptr(b), float(beta)))

@@ -43,6 +43,7 @@ System::~System() {
   if (stream) cudaStreamSynchronize(stream);
   if (sync_ev) cudaEventDestroy(sync_ev);
   if (host_res) pinned_put(host_res);
+  if (umma_err_host) cudaFreeHost(umma_err_host);
 }
 
 // Small pinned host buffers (exact-sum results) are kept in a process-wide free list: freeing
@@ -66,11 +67,12 @@ void pinned_put(uint64_t* p) {
 void host_wait(System& S) {
   if (!S.blocking_sync) {
     CQ_CUDA(cudaStreamSynchronize(S.stream));
-    return;
+  } else {
+    if (!S.sync_ev) CQ_CUDA(cudaEventCreateWithFlags(&S.sync_ev, cudaEventBlockingSync | cudaEventDisableTiming));
+    CQ_CUDA(cudaEventRecord(S.sync_ev, S.stream));
+    CQ_CUDA(cudaEventSynchronize(S.sync_ev));
   }
-  if (!S.sync_ev) CQ_CUDA(cudaEventCreateWithFlags(&S.sync_ev, cudaEventBlockingSync | cudaEventDisableTiming));
-  CQ_CUDA(cudaEventRecord(S.sync_ev, S.stream));
-  CQ_CUDA(cudaEventSynchronize(S.sync_ev));
+  umma_check(S);
 }
 
 // drop-in kernels (one m_kern_max / m_kern_min call): explicit offsets prepared on the host
@@ -262,6 +264,18 @@ int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int
   });
 }
 
+int cq_product_tensor_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* tiles,
+                           int64_t* issued_flops, int* usable) {
+  return guarded([&] {
+    check_sys(sys); check_range(sys, ra); check_range(sys, rb); check_range(sys, rc);
+    CQ_CHECK(mult_type == 1 || mult_type == 2, CQ_ERR_ARG, "mult_type must be 1 or 2");
+    UmmaPlan& U = get_umma_plan(sys->S, mult_type, ra, rb, rc);
+    if (tiles) *tiles = U.n_tiles;
+    if (issued_flops) *issued_flops = U.issued_flops;
+    if (usable) *usable = U.usable ? 1 : 0;
+  });
+}
+
 int cq_matrix_sum(cq_system* sys, int ra, double* a_dev, double alpha, int rb, const double* b_dev, double beta) {
   return guarded([&] {
     check_sys(sys); check_range(sys, ra); check_range(sys, rb);
@@ -336,6 +350,10 @@ int cq_system_set_option(cq_system* sys, int option, int value) {
       sys->S.mult_variant = value;
     } else if (option == CQ_OPT_BLOCKING_SYNC) {
       sys->S.blocking_sync = value != 0;
+    } else if (option == CQ_OPT_MIXED_KERNEL) {
+      CQ_CHECK(value >= -1 && value <= 1, CQ_ERR_ARG,
+               "mixed kernel must be -1 (timed choice), 0 (tcgen05 tiles) or 1 (mma.sync blocks)");
+      sys->S.mixed_kernel = value;
     } else {
       throw Error(CQ_ERR_ARG, "unknown option");
     }

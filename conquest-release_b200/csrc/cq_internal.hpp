@@ -216,6 +216,8 @@ struct MixedPlan {
   int mult_type = 1, ra = -1, rb = -1, rc = -1, out_range = -1;
   int n_groups[4] = {-1, -1, -1, -1};   // groups of 1, 2, 4 and 8 output blocks (-1: not built yet)
   int tuned_g = -1;                 // group size chosen by the autotuner (index into 1, 2, 4, 8)
+  int kernel = -1;                  // 0 = tcgen05 tiles, 1 = per-block mma.sync (-1: not chosen yet)
+  float kernel_ms[2] = {0, 0};      // their timed milliseconds when the choice was made by timing
   float tune_ms[4] = {0, 0, 0, 0};
   int64_t n_pairs = 0, flops = 0;
   DevBuf<int64_t> own_ptr;        // type 2 only (type 1 uses the FP64 plan's lists, already sorted)
@@ -226,6 +228,27 @@ struct MixedPlan {
 };
 
 struct FragBuf { DevBuf<uint4> hi, lo; };
+
+// Dense tensor-core tile of a split-precision product (umma.cu): up to 128 output rows (a run of
+// primary atoms) x up to 128 output columns (a run of the rows' output column atoms), contracted over
+// the cover atoms that occur in the tile's pair lists, packed along K.
+struct UmmaTile {
+  int row_first, n_rows;          // primary atoms [row_first, row_first + n_rows)
+  int col_off, n_cols;            // column atoms col_atoms[col_off, col_off + n_cols)
+  int c_off, n_c;                 // contraction atoms c_atoms / c_koff[c_off, c_off + n_c)
+  int om_off, k_total;            // outmap[om_off + ii * n_cols + jj]; sum of the contraction atoms' block sizes
+  int64_t xp_off, bp_off;         // xpanel[xp_off + c * n_rows + ii], bpanel[bp_off + c * n_cols + jj]
+};
+
+struct UmmaPlan {
+  bool usable = false;            // every block size in 4..128
+  int n_tiles = 0;
+  int64_t flops = 0, n_pairs = 0; // useful work (the FP64 plan's)
+  int64_t issued_flops = 0;       // tensor work issued: 3 MMAs x 2 x 128 x 128 x padded K per tile
+  DevBuf<UmmaTile> tiles;
+  DevBuf<int> col_atoms, c_atoms, c_koff, outmap;
+  DevBuf<long long> xpanel, bpanel;   // first element of each (contraction atom, row / column atom) block, -1: absent
+};
 
 struct AddMap {                   // partner of each block of range A in range B (-1 = none)
   DevBuf<int> partner;
@@ -258,6 +281,11 @@ struct System {
   std::map<std::pair<int, int>, std::unique_ptr<AddMap>> addmaps;
   std::map<std::tuple<int, int, int, int>, std::unique_ptr<MixedPlan>> mplans;
   std::map<std::pair<int, int>, FragBuf> frags;   // (range, slot) fragment buffers of the mixed products
+  std::map<std::tuple<int, int, int, int>, std::unique_ptr<UmmaPlan>> uplans;   // tensor-core tile plans
+  int mixed_kernel = -1;          // split-precision products: 0 = tcgen05 tiles (umma.cu), 1 = mma.sync per block,
+                                  // -1 = the faster of the two, timed per product
+  int* umma_err_host = nullptr;   // mapped host word set by a tensor-core product whose bounded wait ran out
+  int* umma_err_dev = nullptr;
   cudaStream_t stream = nullptr;  // the stream all work of the system is enqueued on
   int uniform_nsf = 0;            // block size when every atom has the same one, else 0
   int n_solvers = 0;              // live LNV solvers built on this system (destroyed before it)
@@ -306,8 +334,16 @@ void generate_SH(System& S, int r, int which, uint64_t seed, double* out);
 void to_fragments(System& S, int r, const double* src, int role_b, int trans, uint4* hi, uint4* lo);
 void launch_mult_tc(System& S, MixedPlan& MP, const uint4* xa_hi, const uint4* xa_lo, const uint4* bb_hi,
                     const uint4* bb_lo, double* out);
-// split-precision mat_mult with the roles of launch_mat_mult (fragments converted per call)
+// split-precision mat_mult with the roles of launch_mat_mult: tcgen05 tiles where every block size is
+// 4..128 (unless the system selects the per-block kernel), else the per-block mma.sync kernel
 void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c);
+
+// umma.cu
+UmmaPlan& get_umma_plan(System& S, int mult_type, int ra, int rb, int rc);
+bool umma_usable(System& S, int mult_type, int ra, int rb, int rc);
+void mat_mult_umma(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c);
+void umma_check(System& S);       // throws CQ_ERR_TIMEOUT if a tensor-core product's wait ran out
+size_t umma_smem_bytes();
 
 // algebra.cu
 void dev_scale(System& S, double* a, int64_t n, double alpha);

@@ -18,6 +18,7 @@
 // mma.m16n8k16, so every fragment is one coalesced 16-byte load per lane.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <climits>
 
 #include "cq_internal.hpp"
@@ -237,8 +238,8 @@ static FragBuf& frag_buffer(System& S, int r, int slot) {
   return f;
 }
 
-void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c) {
-  MixedPlan& MP = get_mixed_plan(S, mult_type, ra, rb, rc);
+static void mat_mult_mma_sync(System& S, MixedPlan& MP, int mult_type, int ra, int rb, int rc, double* a,
+                              const double* b, double* c) {
   int rx = mult_type == 1 ? ra : rc;
   const double* x = mult_type == 1 ? a : c;
   double* out = mult_type == 1 ? c : a;
@@ -247,6 +248,52 @@ void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a,
   to_fragments(S, rx, x, 0, 0, fx.hi.p, fx.lo.p);
   to_fragments(S, rb, b, 1, mult_type == 2 ? 1 : 0, fb.hi.p, fb.lo.p);
   launch_mult_tc(S, MP, fx.hi.p, fx.lo.p, fb.hi.p, fb.lo.p, out);
+}
+
+// Kernel choice of a split-precision product: the system's setting, or (setting -1) the faster of the
+// tcgen05 tiles and the per-block mma.sync kernel, timed on the product's first call (each warm
+// once, then the better of two timed launches each; both write the whole output).
+void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c) {
+  MixedPlan& MP = get_mixed_plan(S, mult_type, ra, rb, rc);
+  const bool tiles_ok = S.max_nsf > 0 && umma_usable(S, mult_type, ra, rb, rc);
+  int k = S.mixed_kernel;
+  if (k == 0 && !tiles_ok) k = 1;
+  if (k < 0) {
+    if (MP.kernel < 0) {
+      if (!tiles_ok) {
+        MP.kernel = 1;
+      } else {
+        cudaEvent_t e0, e1;
+        CQ_CUDA(cudaEventCreate(&e0));
+        CQ_CUDA(cudaEventCreate(&e1));
+        float best[2] = {1e30f, 1e30f};
+        for (int kk = 0; kk < 2; ++kk) {
+          auto run = [&] {
+            if (kk == 0) mat_mult_umma(S, mult_type, ra, rb, rc, a, b, c);
+            else mat_mult_mma_sync(S, MP, mult_type, ra, rb, rc, a, b, c);
+          };
+          run();
+          for (int rep = 0; rep < 2; ++rep) {
+            CQ_CUDA(cudaEventRecord(e0, S.stream));
+            run();
+            CQ_CUDA(cudaEventRecord(e1, S.stream));
+            CQ_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            best[kk] = std::min(best[kk], ms);
+          }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        MP.kernel_ms[0] = best[0];
+        MP.kernel_ms[1] = best[1];
+        MP.kernel = best[0] <= best[1] ? 0 : 1;
+      }
+    }
+    k = MP.kernel;
+  }
+  if (k == 0) mat_mult_umma(S, mult_type, ra, rb, rc, a, b, c);
+  else mat_mult_mma_sync(S, MP, mult_type, ra, rb, rc, a, b, c);
 }
 
 static void launch_tc_g(System& S, MixedPlan& MP, TCArgs M, int gi) {

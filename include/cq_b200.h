@@ -165,6 +165,14 @@ int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64
 int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int* variant, float* ms, int* group,
                       float* group_ms);
 
+/* Tensor-core form of one product (no counterpart in the reference, whose kernels are scalar): the
+ * dense 128 x 128 tiles its split-precision products run on (building their plan on first use),
+ * the tensor work those tiles issue (3 MMAs x 2 x 128 x 128 x the K extent padded to the pipeline's
+ * chunk, per tile), and whether every block size fits the tiles (4..128; usable = 0: the
+ * split-precision products of this system run one padded block per warp instead). */
+int cq_product_tensor_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* tiles,
+                           int64_t* issued_flops, int* usable);
+
 /*
  * Drop-in kernel pair (plugin surface of multiply_kernel_<MULT_KERN>.f90):
  * the argument lists of m_kern_max / m_kern_min
@@ -238,6 +246,11 @@ int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out)
  * spins in cudaStreamSynchronize (default, lowest latency for one solver). */
 #define CQ_OPT_MULT_VARIANT 1
 #define CQ_OPT_BLOCKING_SYNC 2
+/* CQ_OPT_MIXED_KERNEL: kernel of the CQ_PREC_BF16X3 products.  -1 (default) = the faster of the two
+ * below, timed on each product's first call; 0 = dense 128 x 128 tiles on the tcgen05 tensor cores
+ * with TMEM accumulators (every block size 4..128; other systems use 1); 1 = one padded 16 x 16
+ * block per warp-level mma.sync (block sizes up to 16). */
+#define CQ_OPT_MIXED_KERNEL 3
 int cq_system_set_option(cq_system* sys, int option, int value);
 
 /* ------------------------------------------------------------------------ */

@@ -1036,6 +1036,33 @@ static void m_kern_min_default(const KernArgs& K) {
   }
 }
 
+// Work of one partition's kernel call without the arithmetic: the loop structure of the default
+// kernel (multiply_kernel_default.f90:165-222), counting the (k, i, j) triples with a stored result
+// (the ncbeg != 0 test, :198) and their flops 2 nd1 nd2 nd3.  Both mult types share the structure.
+static int64_t g_cnt_triples = 0, g_cnt_flops = 0;
+static void m_kern_count(const KernArgs& K) {
+  const Halo& ah = *K.ahalo; const Halo& ch = *K.chalo; const Trans& at = *K.at;
+  for (int k = 1; k <= ah.nh_part[K.kpart]; ++k) {
+    int k_in_halo = ah.j_beg[K.kpart] + k - 1;
+    int k_in_part = ah.j_seq[k_in_halo];
+    int nbkbeg = K.ibaddr[k_in_part];
+    int nd3 = ah.ndimj[k_in_halo];
+    int nbn = K.nbnab[k_in_part];
+    for (int i = 1; i <= at.n_hnab[k_in_halo]; ++i) {
+      int i_in_prim = at.i_prim[at.i_beg[k_in_halo] + i - 1];
+      int nd1 = ah.ndimi[i_in_prim];
+      size_t icad = (size_t)(i_in_prim - 1) * ch.ni_in_halo;
+      for (int j = 1; j <= nbn; ++j) {
+        int jpart = K.ibpart[nbkbeg + j - 1] + K.k_off;
+        int jh = ch.i_halo[ch.i_hbeg[jpart] + K.ibseq[nbkbeg + j - 1] - 1];
+        if (jh == 0 || ch.i_h2d[icad + jh] == 0) continue;
+        g_cnt_triples += 1;
+        g_cnt_flops += 2ll * nd1 * nd3 * K.bndim2[nbkbeg + j - 1];
+      }
+    }
+  }
+}
+
 // m_kern_max / m_kern_min, ompDoii kernel (multiply_kernel_ompDoii.f90:132-262 and its m_kern_min):
 // the default kernel's arithmetic with `!$omp do` over the primary neighbours i of each k.
 // Different i write different output blocks, so every element sees the default kernel's
@@ -1283,11 +1310,13 @@ static void mat_mult(System& s, int mult_type, int ra, int rb, int rc, double* a
     K.ahalo = &A.halo; K.chalo = &C.halo; K.at = &A.trans;
     return K;
   };
-  if (kernel == 0) {
+  if (kernel == 0 || kernel == 3) {
     for (int kpart = 1; kpart <= np_in_halo; ++kpart) {
       prefetch_part(kpart);
       KernArgs K = make_args(kpart, A.halo.lab_hcover[kpart]);
-      if (mult_type == 1) m_kern_max_default(K); else m_kern_min_default(K);
+      if (kernel == 3) m_kern_count(K);
+      else if (mult_type == 1) m_kern_max_default(K);
+      else m_kern_min_default(K);
     }
   } else {
 #pragma omp parallel default(shared)
@@ -1496,6 +1525,18 @@ int orc_mat_mult(void* h, int mult_type, int ra, int rb, int rc, double* a, int 
   System& s = *(System*)h;
   if (kernel == 1 && !g_dgemm) return 2;
   mat_mult(s, mult_type, ra, rb, rc, a, lena, b, lenb, c, lenc, kernel, nthreads);
+  return 0;
+}
+
+// Triples and flops of one product (no arithmetic): the partition loop of mat_mult with the counting
+// kernel; the operand arrays are scratch copies of the ranges' lengths.
+int orc_product_work(void* h, int mult_type, int ra, int rb, int rc, int64_t* triples, int64_t* flops) {
+  System& s = *(System*)h;
+  std::vector<double> a(std::max<int64_t>(s.ranges[ra].length, 1), 0.0), b(std::max<int64_t>(s.ranges[rb].length, 1), 0.0),
+      c(std::max<int64_t>(s.ranges[rc].length, 1), 0.0);
+  g_cnt_triples = 0; g_cnt_flops = 0;
+  mat_mult(s, mult_type, ra, rb, rc, a.data(), (int)a.size(), b.data(), (int)b.size(), c.data(), (int)c.size(), 3, 0);
+  *triples = g_cnt_triples; *flops = g_cnt_flops;
   return 0;
 }
 

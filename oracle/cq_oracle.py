@@ -54,6 +54,8 @@ def _load():
     lib.orc_mat_mult.restype = c_int
     lib.orc_mat_mult.argtypes = [c_void_p, c_int, c_int, c_int, c_int, P(c_double), c_int, P(c_double), c_int,
                                  P(c_double), c_int, c_int, c_int]
+    lib.orc_product_work.restype = c_int
+    lib.orc_product_work.argtypes = [c_void_p, c_int, c_int, c_int, c_int, P(ctypes.c_int64), P(ctypes.c_int64)]
     lib.orc_matrix_add.argtypes = [c_void_p, c_double, P(c_double), c_int, c_double, P(c_double), c_int]
     lib.orc_matrix_transpose.argtypes = [c_void_p, c_int, P(c_double), P(c_double)]
     lib.orc_matrix_trace.restype = c_double
@@ -165,6 +167,12 @@ class OracleSystem:
                                     k, int(nthreads))
         if st != 0:
             raise RuntimeError("oracle mat_mult failed (%d)" % st)
+
+    def product_work(self, mult_type, ra, rb, rc):
+        """(triples, flops) of one product: the (k, i, j) triples with a stored result and 2 nd1 nd2 nd3 each."""
+        t, f = ctypes.c_int64(), ctypes.c_int64()
+        self._lib.orc_product_work(self._h, mult_type, ra, rb, rc, ctypes.byref(t), ctypes.byref(f))
+        return t.value, f.value
 
     def matrix_add(self, alpha, a, ra, beta, b, rb):
         self._lib.orc_matrix_add(self._h, float(alpha), _dp(a), ra, float(beta), _dp(b), rb)

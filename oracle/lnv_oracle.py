@@ -222,6 +222,10 @@ class OracleLNV:
         self.phi = self.temp("L")
         self.delta_e = 0.0                  # `save` variable of FindMinDM
         self.n_products = 0
+        self.flops = 0                      # algorithmic flops of the products run so far
+        self._work = {}
+        # optional: a callable run before every product (a bounded sample stops the chain by raising)
+        self.before_product = None
         self.log = []
         self.rlog = []          # every trace / product-trace value in call order (chain comparison)
         # minE.MixedLSelfConsistent: callable(K values) -> new H values, run by lateDM
@@ -234,7 +238,13 @@ class OracleLNV:
 
     def product(self, A, B, C, mult):
         t, ra, rb, rc = MULTS[mult]
+        if self.before_product is not None:
+            self.before_product(self)
         self.n_products += 1
+        key = (t, ra, rb, rc)
+        if key not in self._work:
+            self._work[key] = self.o.product_work(t, self.ridx[ra], self.ridx[rb], self.ridx[rc])[1]
+        self.flops += self._work[key]
         if t == 1:
             assert A.rng == ra and B.rng == rb and C.rng == rc, mult
             self.o.mat_mult(1, self.ridx[ra], self.ridx[rb], self.ridx[rc], A.v, B.v, C.v, kernel=self.kernel,

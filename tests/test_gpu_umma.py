@@ -1,0 +1,127 @@
+"""Split-precision block products on the tcgen05 tensor cores (dense 128 x 128 tiles, TMEM
+accumulators) against the oracle's FP64 default kernel.
+
+Every operand value is split into two bf16 parts (hi + lo, about 16 significant bits) and a block
+product is hi.hi + hi.lo + lo.hi with FP32 accumulation, so per output element
+    |got - ref| <= 2^-14 * sum |a| |b| over the element's terms
+(the same bound as the per-block mma.sync kernel).  The output is fully overwritten: blocks with no
+terms come out as zeros, never as the NaNs the output held before.
+"""
+import numpy as np
+import pytest
+
+import blockmaps as bm
+import systems
+from cq_b200 import inputs
+from cq_oracle import OracleSystem
+
+pytestmark = pytest.mark.gpu
+
+TOL = 2.0 ** -14
+
+
+def _run(o, g, t, ia, ib, ic, bls_a, bls_b, bls_c, seed, kernel=0):
+    """One product on both sides; returns (got, ref, sum |a||b| bound)."""
+    import cq_b200
+    g.set_mixed_kernel(kernel)
+    b = inputs.random_blocks(bls_b, seed, inputs.TAG_RANDOM_B)
+    if t == 1:
+        a = inputs.random_blocks(bls_a, seed, inputs.TAG_RANDOM_A)
+        ref = np.zeros(bls_c.length); o.mat_mult(1, ia, ib, ic, a, b, ref)
+        bound = np.zeros(bls_c.length); o.mat_mult(1, ia, ib, ic, np.abs(a), np.abs(b), bound)
+        got = np.full(bls_c.length, np.nan)
+        g.mat_mult_host(1, ia, ib, ic, a, b, got, precision=cq_b200.PREC_BF16X3)
+    else:
+        c = inputs.random_blocks(bls_c, seed + 1, inputs.TAG_RANDOM_A)
+        ref = np.zeros(bls_a.length); o.mat_mult(2, ia, ib, ic, ref, b, c)
+        bound = np.zeros(bls_a.length); o.mat_mult(2, ia, ib, ic, bound, np.abs(b), np.abs(c))
+        got = np.full(bls_a.length, np.nan)
+        g.mat_mult_host(2, ia, ib, ic, got, b, c, precision=cq_b200.PREC_BF16X3)
+    return got, ref, bound
+
+
+def _assert_bound(got, ref, bound):
+    assert not np.any(np.isnan(got)), "output blocks left unwritten"
+    err = np.abs(got - ref)
+    worst = np.max(err / np.maximum(bound, 1e-300))
+    assert np.all(err <= TOL * bound + 1e-300), "worst error / sum|a||b| = %.3g" % worst
+    assert err.max() > 0          # it really ran in reduced precision
+
+
+@pytest.fixture(scope="module")
+def cfg1():
+    import cq_b200
+    coords, cell, nsf, rc = systems.config1()
+    o = OracleSystem(coords, cell, nsf, rc)
+    g = cq_b200.System(coords, cell, nsf, rc)
+    bls = [bm.oracle_blocklist(o, r, coords, cell) for r in range(3)]
+    return o, g, bls
+
+
+@pytest.fixture(scope="module")
+def cfg2():
+    import cq_b200
+    coords, cell, nsf = systems.config2()
+    rng = systems.lnv_ranges()
+    names = list(rng.keys())
+    o = OracleSystem(coords, cell, nsf, list(rng.values()))
+    g = cq_b200.System(coords, cell, nsf, list(rng.values()))
+    bls = {n: bm.oracle_blocklist(o, i, coords, cell) for i, n in enumerate(names)}
+    return o, g, bls, {n: i for i, n in enumerate(names)}
+
+
+@pytest.mark.parametrize("kernel", [0, 1])
+@pytest.mark.parametrize("mult_type", [1, 2])
+def test_dzp_products_within_split_bound(cfg1, mult_type, kernel):
+    """216-atom Si, 13x13 blocks, A 8 / B 12 / C 20 bohr: tcgen05 tiles (0) and per-block mma.sync (1)."""
+    o, g, bls = cfg1
+    got, ref, bound = _run(o, g, mult_type, 0, 1, 2, bls[0], bls[1], bls[2], 41 + mult_type, kernel)
+    _assert_bound(got, ref, bound)
+
+
+def test_tile_plan_accounts_for_the_work(cfg1):
+    """The tiles cover the product: the issued tensor work is at least the three split terms of every
+    useful triple, and the plan is usable for 13x13 blocks."""
+    o, g, bls = cfg1
+    tiles, issued, usable = g.product_tensor_work(1, 0, 1, 2)
+    triples, flops = g.product_work(1, 0, 1, 2)
+    assert usable and tiles > 0
+    assert issued >= 3 * flops
+    # 128 x 128 tiles, K padded to 32: the tile count bounds the issued work from above
+    assert issued <= 3 * 2 * 128 * 128 * tiles * (triples * 13 // max(tiles, 1) + 32 * tiles)
+
+
+SZ_PRODUCTS = [(1, "L", "S", "LS"), (1, "LS", "L", "LSL"), (2, "L", "LS", "LSL"), (2, "H", "LS", "LSL"),
+               (1, "LS", "S", "SLS"), (2, "L", "T", "TL")]
+
+
+@pytest.mark.parametrize("prod", SZ_PRODUCTS)
+def test_sz_products_within_split_bound(cfg2, prod):
+    """512-atom Si, 4x4 blocks (32 atoms per 128-row tile), products of the LNV chain, both mult types."""
+    o, g, bls, idx = cfg2
+    t, ra, rb, rc = prod
+    got, ref, bound = _run(o, g, t, idx[ra], idx[rb], idx[rc], bls[ra], bls[rb], bls[rc], 51)
+    _assert_bound(got, ref, bound)
+    assert g.product_tensor_work(t, idx[ra], idx[rb], idx[rc])[2]
+
+
+@pytest.mark.parametrize("mult_type", [1, 2])
+def test_mixed_block_sizes_within_split_bound(mult_type):
+    """Atoms with 4 and 13 orbitals in one system: atoms of both sizes packed into the same tiles."""
+    import cq_b200
+    coords, cell = inputs.diamond_si(2, sigma=0.05, seed=21)
+    nsf = np.where(np.arange(len(coords)) % 3 == 0, 13, 4).astype(np.int32)
+    rc = [6.0, 8.0, 14.0]
+    o = OracleSystem(coords, cell, nsf, rc)
+    g = cq_b200.System(coords, cell, nsf, rc)
+    bls = [bm.oracle_blocklist(o, r, coords, cell) for r in range(3)]
+    got, ref, bound = _run(o, g, mult_type, 0, 1, 2, bls[0], bls[1], bls[2], 61)
+    _assert_bound(got, ref, bound)
+
+
+def test_repeatable_bits(cfg1):
+    """The tiles accumulate in a fixed order: two launches give the same bits."""
+    o, g, bls = cfg1
+    got1, _, _ = _run(o, g, 1, 0, 1, 2, bls[0], bls[1], bls[2], 71)
+    got2, _, _ = _run(o, g, 1, 0, 1, 2, bls[0], bls[1], bls[2], 71)
+    assert np.array_equal(got1, got2)
