@@ -230,24 +230,27 @@ struct MixedPlan {
 struct FragBuf { DevBuf<uint4> hi, lo; };
 
 // Dense tensor-core tile of a split-precision product (umma.cu): up to 128 output rows (a run of
-// primary atoms) x up to 128 output columns (a run of the rows' output column atoms), contracted over
-// the cover atoms that occur in the tile's pair lists, packed along K.
+// primary atoms) x one column chunk (a run of up to 128 orbitals of cover atoms), contracted over the
+// units (runs of cover atoms of up to 16 orbitals) that its pair lists use.
 struct UmmaTile {
   int row_first, n_rows;          // primary atoms [row_first, row_first + n_rows)
-  int col_off, n_cols;            // column atoms col_atoms[col_off, col_off + n_cols)
-  int c_off, n_c;                 // contraction atoms c_atoms / c_koff[c_off, c_off + n_c)
-  int om_off, k_total;            // outmap[om_off + ii * n_cols + jj]; sum of the contraction atoms' block sizes
-  int64_t xp_off, bp_off;         // xpanel[xp_off + c * n_rows + ii], bpanel[bp_off + c * n_cols + jj]
+  int n_cols;                     // atoms of the column chunk
+  int row_tab, col_tab;           // offsets of the 128-entry row tables of the row group and the chunk
+  int om_off;                     // outmap[om_off + ii * n_cols + jj]: output block or -1
+  int u_off, n_u;                 // unit entries units[u_off, u_off + n_u): (X slab, B slab)
 };
 
 struct UmmaPlan {
-  bool usable = false;            // every block size in 4..128
+  bool usable = false;            // every block size in 4..16
   int n_tiles = 0;
   int64_t flops = 0, n_pairs = 0; // useful work (the FP64 plan's)
-  int64_t issued_flops = 0;       // tensor work issued: 3 MMAs x 2 x 128 x 128 x padded K per tile
+  int64_t issued_flops = 0;       // tensor work issued: 3 MMAs x 2 x 128 x 128 x 16 per unit of every tile
+  int64_t n_xslabs = 0, n_bslabs = 0;
   DevBuf<UmmaTile> tiles;
-  DevBuf<int> col_atoms, c_atoms, c_koff, outmap;
-  DevBuf<long long> xpanel, bpanel;   // first element of each (contraction atom, row / column atom) block, -1: absent
+  DevBuf<int2> units;
+  DevBuf<unsigned int> rtabs, ktabs;   // row tables (row groups, column chunks); K tables of the units
+  DevBuf<int> outmap, xtab, btab, xs_rtab, xs_unit, bs_rtab, bs_unit;
+  DevBuf<uint4> xslabs, bslabs;   // packed bf16 operands, 8 KB per slab, rewritten by every product call
 };
 
 struct AddMap {                   // partner of each block of range A in range B (-1 = none)

@@ -1,25 +1,31 @@
-// Split-precision block products on the 5th-generation tensor cores (tcgen05.mma, TMEM accumulators).
+// Split-precision block products on the 5th-generation tensor cores (tcgen05.mma, TMEM accumulators,
+// operand tiles staged by the bulk-copy (TMA) engine).
 //
 // The atom-block product C(i,j) = sum_k A(i,k) B(k,j) (type 1, src/multiply_kernel_default.f90:204-214;
 // type 2 a(i,k) = sum_j c(i,j) b(k,j)^T, :390-402) is regrouped into dense tiles:
-//   rows        a run of consecutive primary atoms whose block sizes add up to at most 128 (M = 128),
-//   columns     a run of output column atoms (the output range's cover atoms of those rows, in cover
-//               order) adding up to at most kNT orbitals (N = kNT),
-//   contraction the cover atoms k (type 1) or j (type 2) that occur in the tile's pair lists, packed
-//               back to back along K (no padding between atoms).
-// Each tile is one CTA.  Eight producer warps gather the FP64 blocks of a K chunk (kKC orbitals)
-// from HBM/L2, split every value v = hi + lo into two bf16 parts (hi = bf16(v), lo = bf16(v - hi),
-// about 16 significant bits) and store them in shared memory in the tensor core's K-major canonical
-// layout (8-row x 16-byte core matrices, no swizzle); absent blocks are stored as zeros.  One thread
-// issues per 16-wide K step the three MMAs lo.hi + hi.lo + hi.hi (kind::f16, bf16 inputs, FP32
-// accumulation) into a 128 x kNT FP32 accumulator in tensor memory; a tcgen05.commit per chunk
-// frees its shared-memory stage.  Four warps then read the accumulator back with tcgen05.ld and
-// write every stored output block of the tile as FP64 (the whole block is overwritten, as the FP64
-// kernels do).  Pairs absent from the pair lists contribute zero blocks, so the tile computes exactly
-// the sum over the (i, k, j) triples of the reference kernel, in a different order and precision.
+//   rows        a run of consecutive primary atoms whose block sizes add up to at most 128 (M = 128);
+//   columns     a column chunk: a run of consecutive cover atoms adding up to at most 128 orbitals
+//               (N = 128), the same chunks for every row group;
+//   contraction units: runs of consecutive cover atoms adding up to at most 16 orbitals (one
+//               16-wide MMA step each: four 4x4 atoms, or one 13x13 atom padded to 16); a tile
+//               contracts over the units that hold a contraction atom (k for type 1, j for type 2)
+//               of its pair lists.
+// Before each product, two packing kernels write the operands once as bf16 "slabs" in the tensor
+// core's K-major shared-memory layout (8-row x 16-byte core matrices, no swizzle): an X slab per
+// (row group, unit) holds the first operand's 128 rows x 16 K, a B slab per (unit, column chunk)
+// the second operand's 128 columns x 16 K, each as a hi part (bf16(v)) and a lo part (bf16(v - hi)),
+// about 16 significant bits; absent blocks are zeros.
+// The product kernel is one CTA per tile.  One thread moves the slabs of each pipeline stage into
+// shared memory with cp.async.bulk (no multicast; 16 KB per unit, completion counted on an mbarrier),
+// one thread issues per unit the three MMAs lo.hi + hi.lo + hi.hi (kind::f16, bf16 inputs, FP32
+// accumulation) into a 128 x 128 FP32 accumulator in tensor memory, a tcgen05.commit per stage frees
+// it, and four warps read the accumulator back with tcgen05.ld and write every stored output block of
+// the tile as FP64 (the whole block is overwritten, as the FP64 kernels do).  Pairs absent from the
+// pair lists contribute zero blocks, so a tile computes exactly the sums over the (i, k, j) triples of
+// the reference kernel, in a different order and precision.
 //
 // Every wait on an mbarrier is bounded (about one second of GPU time); a wait that runs out sets an
-// error word in mapped host memory, the kernel still drains the MMAs it issued before releasing
+// error word in mapped host memory, the kernel drains the copies and MMAs it issued before it releases
 // the tensor memory, and the host reports CQ_ERR_TIMEOUT.
 #include <cuda_bf16.h>
 
@@ -34,43 +40,34 @@ namespace {
 
 constexpr int kM = 128;             // accumulator rows (TMEM lanes)
 constexpr int kNT = 128;            // accumulator columns
-constexpr int kKC = 32;             // K orbitals per pipeline stage (two 16-wide MMA steps)
+constexpr int kUK = 16;             // K orbitals of one contraction unit (one MMA step)
+constexpr int kUnitsPerStage = 2;
 constexpr int kStages = 3;
-constexpr int kProducerWarps = 8;
-constexpr int kProducers = 32 * kProducerWarps;
-constexpr int kThreads = kProducers + 32;   // + one warp: TMEM allocation and MMA issue
-constexpr int kMaxRowAtoms = 32;    // block sizes >= 4: at most 32 atoms per 128 rows / columns
+constexpr int kMaxAtoms = 32;       // atoms per row group / column chunk (block sizes >= 4)
+constexpr int kMaxUnitAtoms = 4;
 constexpr int kMinNd = 4;
-constexpr int kMaxChunkAtoms = kKC / kMinNd + 2;
 constexpr uint32_t kTmemCols = kNT;
+constexpr int kThreads = 192;       // warps 0-3 epilogue, warp 4 bulk copies, warp 5 TMEM + MMA
 
-// operand tiles of one stage: A (rows x K) and B (columns x K), bf16 hi and lo parts, K-major core matrices
-constexpr int kTileBytesA = kM * kKC * 2;
-constexpr int kTileBytesB = kNT * kKC * 2;
-constexpr int kStageBytes = 2 * kTileBytesA + 2 * kTileBytesB;
-
-struct ChunkMeta {
-  long long xo[kMaxChunkAtoms][kMaxRowAtoms];   // first element of X(i, c) for the chunk's atoms c (-1: absent)
-  long long bo[kMaxChunkAtoms][kMaxRowAtoms];   // first element of the B block of (c, column atom)
-  int cnd[kMaxChunkAtoms];                      // block size of each chunk atom
-  unsigned short kmap[kKC];                     // K position -> (chunk atom, orbital), 0xffff = padding
-};
+// one slab: hi part then lo part, each [K group (2)][row group (16)][8 rows x 16 bytes]
+constexpr int kSlabHalf = kM * kUK * 2;          // 4 KB
+constexpr int kSlabBytes = 2 * kSlabHalf;        // 8 KB
+static_assert(kNT == kM, "B slabs use the X slab layout");
+// stage: A hi, A lo, B hi, B lo regions of kUnitsPerStage slab halves each
+constexpr int kRegion = kUnitsPerStage * kSlabHalf;
+constexpr int kStageBytes = 4 * kRegion;
 
 struct Smem {
   alignas(1024) unsigned char stage[kStages][kStageBytes];
-  ChunkMeta meta[2];
   unsigned int rowtab[kM];          // row m -> ii | n1 << 8 | nd << 16 (0xffffffff: unused row)
   unsigned int coltab[kNT];         // column -> jj | nn << 8 | nd << 16
   unsigned long long full[kStages], empty[kStages], accfull;
   unsigned int tmem_base;
   int abort;
 };
-
-// two CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA), so that one CTA's epilogue and
-// set-up overlap the other's MMAs; two 128-column accumulators fit the 512 TMEM columns with room
+// two CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA): one CTA's set-up and epilogue
+// overlap the other's MMAs; their two 128-column accumulators fit the 512 TMEM columns
 static_assert(sizeof(Smem) + 1024 <= 113 * 1024, "shared memory of the tensor-core product exceeds half an SM");
-
-__device__ const double g_umma_zero = 0.0;   // load target of absent blocks (the loads stay unconditional)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -83,8 +80,8 @@ __device__ __forceinline__ uint64_t global_ns() {
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
-__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 // Wait for the phase with the given parity to complete; false once the CTA has aborted, or after
 // `limit_ns` of GPU time (then the error word is set and the CTA aborts).
@@ -115,23 +112,16 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t pari
   }
 }
 
-// named barrier of the producer warps that also ORs a flag over them (a uniform decision)
-__device__ __forceinline__ bool producers_any(bool flag) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\t"
-      "setp.ne.b32 p, %1, 0;\n\t"
-      "bar.red.or.pred q, 1, %2, p;\n\t"
-      "selp.u32 %0, 1, 0, q;\n\t}\n"
-      : "=r"(r)
-      : "r"((uint32_t)flag), "n"(kProducers)
-      : "memory");
-  return r != 0;
+// bulk copy global -> shared memory (no multicast), completion counted in bytes on `bar`
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // shared-memory matrix descriptor: K-major, no swizzle; lbo = byte distance of core matrices along K,
 // sbo = byte distance of 8-row groups along M / N; bits 46-47 = 1 (tcgen05 descriptor version)
@@ -167,8 +157,8 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// byte offset of the 16-byte K group g of row r in a K-major operand tile of kKC columns
-__device__ __forceinline__ uint32_t core_off(int r, int g) { return ((r >> 3) * (kKC / 8) + g) * 128 + (r & 7) * 16; }
+// byte offset of (row r, K group g) within a slab half
+__host__ __device__ __forceinline__ uint32_t slab_off(int r, int g) { return g * 2048 + (r >> 3) * 128 + (r & 7) * 16; }
 
 // v = hi + lo for 8 values: two 16-byte rows of bf16 (element e at bytes 2e, 2e+1)
 __device__ __forceinline__ void split8(const float (&v)[8], uint4& hi, uint4& lo) {
@@ -187,22 +177,65 @@ __device__ __forceinline__ void split8(const float (&v)[8], uint4& hi, uint4& lo
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// packing: one CTA of 256 threads per slab, one thread per (row, K group of 8)
+//   rtabs: row r of the slab -> atom position | orbital << 8 | block size << 16 (0xffffffff: empty)
+//   ktabs: K position of the slab's unit -> atom position | orbital << 8 | block size << 16
+//   btab:  [slab][atom of the unit (4)][row atom (32)] -> block index or -1
+// The value at (row r, K k) is the block (row atom, unit atom) at element (orbital_r, orbital_k),
+// column-major: k_fastest = 1 puts the K orbital fastest (leading dimension = the K atom's block
+// size), k_fastest = 0 the row orbital (leading dimension = the row atom's block size).
+// ---------------------------------------------------------------------------
+struct PackArgs {
+  const int* __restrict__ slab_rtab;  // per slab: offset of its 128-entry row table
+  const int* __restrict__ slab_unit;  // per slab: its unit
+  const unsigned int* __restrict__ rtabs;
+  const unsigned int* __restrict__ ktabs;   // [unit][16]
+  const int* __restrict__ btab;
+  const int64_t* __restrict__ elem;
+  const double* __restrict__ src;
+  uint4* __restrict__ out;            // [slab][512] (8 KB)
+  int k_fastest;
+};
+
+__global__ void __launch_bounds__(256) k_umma_pack(PackArgs A) {
+  const int s = blockIdx.x, t = threadIdx.x;
+  const int r = t & 127, g = t >> 7;
+  const unsigned int ri = A.rtabs[A.slab_rtab[s] + r];
+  const unsigned int* kt = A.ktabs + (size_t)A.slab_unit[s] * kUK + g * 8;
+  float v[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    double val = 0.0;
+    const unsigned int ki = kt[e];
+    if (ri != 0xffffffffu && ki != 0xffffffffu) {
+      const int ra = ri & 0xff, ro = (ri >> 8) & 0xff, rnd = ri >> 16;
+      const int ka = ki & 0xff, ko = (ki >> 8) & 0xff, knd = ki >> 16;
+      const int blk = A.btab[(size_t)s * (kMaxUnitAtoms * kMaxAtoms) + ka * kMaxAtoms + ra];
+      if (blk >= 0) val = __ldg(A.src + A.elem[blk] + (A.k_fastest ? ko + (int64_t)knd * ro : ro + (int64_t)rnd * ko));
+    }
+    v[e] = (float)val;
+  }
+  uint4 hi, lo;
+  split8(v, hi, lo);
+  unsigned char* base = reinterpret_cast<unsigned char*>(A.out + (size_t)s * (kSlabBytes / 16));
+  *reinterpret_cast<uint4*>(base + slab_off(r, g)) = hi;
+  *reinterpret_cast<uint4*>(base + kSlabHalf + slab_off(r, g)) = lo;
+}
+
+// ---------------------------------------------------------------------------
+// the product kernel: one CTA per tile
+// ---------------------------------------------------------------------------
 struct UmmaArgs {
   const UmmaTile* __restrict__ tiles;
-  const int* __restrict__ col_atoms;
-  const int* __restrict__ c_atoms;
-  const int* __restrict__ c_koff;
-  const long long* __restrict__ xpanel;   // first element of X(i, c) per (contraction atom, row atom), -1: absent
-  const long long* __restrict__ bpanel;   // first element of the B block per (contraction atom, column atom)
+  const int2* __restrict__ units;     // per tile unit entry: (X slab, B slab)
+  const unsigned int* __restrict__ rtabs;   // row tables of the row groups and of the column chunks
   const int* __restrict__ outmap;
-  const int* __restrict__ prim_nsf;
-  const int* __restrict__ cover_nsf;
+  const uint4* __restrict__ xslabs;
+  const uint4* __restrict__ bslabs;
   const int64_t* __restrict__ o_elem;
-  const double* __restrict__ x;
-  const double* __restrict__ b;
   double* __restrict__ out;
-  int type;
-  int* err;                        // mapped host word: a bounded wait ran out
+  int* err;                           // mapped host word: a bounded wait ran out
 };
 
 __global__ void __launch_bounds__(kThreads, 2) k_mult_umma(UmmaArgs P) {
@@ -210,166 +243,76 @@ __global__ void __launch_bounds__(kThreads, 2) k_mult_umma(UmmaArgs P) {
   Smem& sm = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const UmmaTile T = P.tiles[blockIdx.x];
-  const int nchunk = (T.k_total + kKC - 1) / kKC;
+  const int nstage = (T.n_u + kUnitsPerStage - 1) / kUnitsPerStage;
 
-  // ---- set-up: barriers, TMEM, row / column / output tables of the tile
-  if (tid == kProducers) {
-    for (int s = 0; s < kStages; ++s) { mbar_init(&sm.full[s], kProducers); mbar_init(&sm.empty[s], 1); }
+  // ---- set-up: barriers, TMEM, row and column tables of the tile
+  if (tid == 128) {
+    for (int s = 0; s < kStages; ++s) { mbar_init(&sm.full[s], 1); mbar_init(&sm.empty[s], 1); }
     mbar_init(&sm.accfull, 1);
     sm.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == kProducerWarps) {
+  if (warp == 5) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem_base)),
                  "r"(kTmemCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  for (int m = tid; m < kM; m += kThreads) {
-    unsigned int v = 0xffffffffu;
-    int off = 0;
-    for (int ii = 0; ii < T.n_rows; ++ii) {
-      const int nd = P.prim_nsf[T.row_first + ii];
-      if (m < off + nd) { v = (unsigned)ii | ((unsigned)(m - off) << 8) | ((unsigned)nd << 16); break; }
-      off += nd;
-    }
-    sm.rowtab[m] = v;
-  }
-  for (int n = tid; n < kNT; n += kThreads) {
-    unsigned int v = 0xffffffffu;
-    int off = 0;
-    for (int jj = 0; jj < T.n_cols; ++jj) {
-      const int nd = P.cover_nsf[P.col_atoms[T.col_off + jj]];
-      if (n < off + nd) { v = (unsigned)jj | ((unsigned)(n - off) << 8) | ((unsigned)nd << 16); break; }
-      off += nd;
-    }
-    sm.coltab[n] = v;
-  }
+  if (tid < kM) sm.rowtab[tid] = P.rtabs[T.row_tab + tid];
+  for (int n = tid; n < kNT; n += kThreads) sm.coltab[n] = P.rtabs[T.col_tab + n];
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sm.tmem_base;
 
-  if (warp < kProducerWarps) {
-    // ---- producers: gather, split and store one K chunk per stage.  The metadata of chunk c + 1
-    // (element offsets of its blocks, K map) is loaded while chunk c's values are in flight, and
-    // every thread issues all its value loads of a chunk before it uses any of them.
-    int cur = 0;                                     // first contraction atom overlapping the next chunk
-    auto load_meta = [&](int c, ChunkMeta& M) {
-      const int k0 = c * kKC;
-      while (cur + 1 < T.n_c && __ldg(P.c_koff + T.c_off + cur + 1) <= k0) ++cur;
-      int nca = 0;                                   // atoms overlapping [k0, k0 + kKC)
-      while (cur + nca < T.n_c && nca < kMaxChunkAtoms && __ldg(P.c_koff + T.c_off + cur + nca) < k0 + kKC) ++nca;
-      const int nrc = T.n_rows + T.n_cols;
-      for (int e = tid; e < nca * nrc; e += kProducers) {
-        const int la = e / nrc, r = e - la * nrc;
-        const int64_t cc = cur + la;
-        if (r < T.n_rows) M.xo[la][r] = __ldg(P.xpanel + T.xp_off + cc * T.n_rows + r);
-        else M.bo[la][r - T.n_rows] = __ldg(P.bpanel + T.bp_off + cc * T.n_cols + (r - T.n_rows));
-      }
-      if (tid < nca) M.cnd[tid] = P.cover_nsf[P.c_atoms[T.c_off + cur + tid]];
-      if (tid < kKC) {
-        const int kk = k0 + tid;
-        unsigned short v = 0xffff;
-        if (kk < T.k_total) {
-          for (int la = nca - 1; la >= 0; --la) {
-            const int ko = __ldg(P.c_koff + T.c_off + cur + la);
-            if (ko <= kk) { v = (unsigned short)(la | ((kk - ko) << 8)); break; }
-          }
-        }
-        M.kmap[tid] = v;
-      }
-    };
-    constexpr int kItems = (kM + kNT) * (kKC / 8) / kProducers;   // items per thread per chunk
-    static_assert((kM + kNT) * (kKC / 8) % kProducers == 0, "items must divide evenly over the producers");
-    if (nchunk > 0) load_meta(0, sm.meta[0]);
-    producers_any(false);
-    for (int c = 0; c < nchunk; ++c) {
-      const int s = c % kStages;
-      const ChunkMeta& M = sm.meta[c & 1];
-      // the stage is free once the MMAs that read it (chunk c - kStages) have completed
-      const bool ok = c < kStages || mbar_wait(&sm.empty[s], ((c / kStages) - 1) & 1, P.err, &sm.abort);
-      // items: A rows x 4 K groups, then B columns x 4 K groups; consecutive threads take consecutive rows
-      double v[kItems][8];
-#pragma unroll
-      for (int q = 0; q < kItems; ++q) {
-        const int it = tid + q * kProducers;
-        const bool isA = it < kM * (kKC / 8);
-        const int j = isA ? it : it - kM * (kKC / 8);
-        const int rows = isA ? kM : kNT;
-        const int r = j % rows, g = j / rows;
-        const unsigned int info = isA ? sm.rowtab[r] : sm.coltab[r];
-        const int idx = info & 0xff, pos = (info >> 8) & 0xff, nd = info >> 16;
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const unsigned short km = M.kmap[g * 8 + e];
-          const double* p = &g_umma_zero;
-          if (info != 0xffffffffu && km != 0xffff) {
-            const int la = km & 0xff, n = km >> 8;
-            if (isA) {
-              const long long o = M.xo[la][idx];
-              if (o >= 0) p = P.x + o + pos + (int64_t)nd * n;
-            } else {
-              const long long o = M.bo[la][idx];
-              if (o >= 0) p = P.b + o + (P.type == 1 ? n + (int64_t)M.cnd[la] * pos : pos + (int64_t)nd * n);
-            }
-          }
-          v[q][e] = __ldg(p);
+  if (warp == 4) {
+    if (lane == 0) {
+      // ---- bulk copies: the X and B slabs of each stage's units
+      for (int c = 0; c < nstage; ++c) {
+        const int s = c % kStages;
+        if (c >= kStages && !mbar_wait(&sm.empty[s], ((c / kStages) - 1) & 1, P.err, &sm.abort)) break;
+        const int u0 = c * kUnitsPerStage, nu = min(kUnitsPerStage, T.n_u - u0);
+        mbar_expect_tx(&sm.full[s], (uint32_t)(nu * 2 * kSlabBytes));
+        unsigned char* st = sm.stage[s];
+        for (int u = 0; u < nu; ++u) {
+          const int2 e = P.units[T.u_off + u0 + u];
+          const unsigned char* xs = reinterpret_cast<const unsigned char*>(P.xslabs) + (size_t)e.x * kSlabBytes;
+          const unsigned char* bs = reinterpret_cast<const unsigned char*>(P.bslabs) + (size_t)e.y * kSlabBytes;
+          bulk_g2s(st + 0 * kRegion + u * kSlabHalf, xs, kSlabHalf, &sm.full[s]);
+          bulk_g2s(st + 1 * kRegion + u * kSlabHalf, xs + kSlabHalf, kSlabHalf, &sm.full[s]);
+          bulk_g2s(st + 2 * kRegion + u * kSlabHalf, bs, kSlabHalf, &sm.full[s]);
+          bulk_g2s(st + 3 * kRegion + u * kSlabHalf, bs + kSlabHalf, kSlabHalf, &sm.full[s]);
         }
       }
-      if (c + 1 < nchunk) load_meta(c + 1, sm.meta[(c + 1) & 1]);
-      unsigned char* st = sm.stage[s];
-#pragma unroll
-      for (int q = 0; q < kItems; ++q) {
-        const int it = tid + q * kProducers;
-        const bool isA = it < kM * (kKC / 8);
-        const int j = isA ? it : it - kM * (kKC / 8);
-        const int rows = isA ? kM : kNT;
-        const int r = j % rows, g = j / rows;
-        float f[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) f[e] = (float)v[q][e];
-        uint4 hi, lo;
-        split8(f, hi, lo);
-        unsigned char* base = st + (isA ? 0 : 2 * kTileBytesA);
-        const int tb = isA ? kTileBytesA : kTileBytesB;
-        *reinterpret_cast<uint4*>(base + core_off(r, g)) = hi;
-        *reinterpret_cast<uint4*>(base + tb + core_off(r, g)) = lo;
-      }
-      fence_async_smem();
-      mbar_arrive(&sm.full[s]);
-      // publishes chunk c + 1's metadata; stops every producer together once a wait has failed
-      if (producers_any(!ok)) break;
     }
-  } else if (lane == 0) {
-    // ---- MMA issue (one thread)
-    constexpr uint32_t idesc = idesc_bf16(kM, kNT);
-    int c = 0;
-    for (; c < nchunk; ++c) {
-      const int s = c % kStages;
-      if (!mbar_wait(&sm.full[s], (c / kStages) & 1, P.err, &sm.abort)) break;
-      tc_fence_after();
-      const uint32_t a_hi = smem_u32(sm.stage[s]), a_lo = a_hi + kTileBytesA;
-      const uint32_t b_hi = a_hi + 2 * kTileBytesA, b_lo = b_hi + kTileBytesB;
-#pragma unroll
-      for (int ks = 0; ks < kKC / 16; ++ks) {
-        const uint32_t ko = ks * 256;            // two 16-byte K groups per 16-wide step
-        const uint32_t sbo = (kKC / 8) * 128;
-        const uint64_t dah = smem_desc(a_hi + ko, 128, sbo), dal = smem_desc(a_lo + ko, 128, sbo);
-        const uint64_t dbh = smem_desc(b_hi + ko, 128, sbo), dbl = smem_desc(b_lo + ko, 128, sbo);
-        umma_bf16(tmem, dal, dbh, idesc, (c > 0 || ks > 0) ? 1u : 0u);
-        umma_bf16(tmem, dah, dbl, idesc, 1u);
-        umma_bf16(tmem, dah, dbh, idesc, 1u);
+  } else if (warp == 5) {
+    if (lane == 0) {
+      // ---- MMA issue (one thread)
+      constexpr uint32_t idesc = idesc_bf16(kM, kNT);
+      for (int c = 0; c < nstage; ++c) {
+        const int s = c % kStages;
+        if (!mbar_wait(&sm.full[s], (c / kStages) & 1, P.err, &sm.abort)) break;
+        tc_fence_after();
+        const uint32_t base = smem_u32(sm.stage[s]);
+        const int nu = min(kUnitsPerStage, T.n_u - c * kUnitsPerStage);
+        for (int u = 0; u < nu; ++u) {
+          const uint32_t o = u * kSlabHalf;
+          const uint64_t dah = smem_desc(base + 0 * kRegion + o, 2048, 128);
+          const uint64_t dal = smem_desc(base + 1 * kRegion + o, 2048, 128);
+          const uint64_t dbh = smem_desc(base + 2 * kRegion + o, 2048, 128);
+          const uint64_t dbl = smem_desc(base + 3 * kRegion + o, 2048, 128);
+          umma_bf16(tmem, dal, dbh, idesc, (c > 0 || u > 0) ? 1u : 0u);
+          umma_bf16(tmem, dah, dbl, idesc, 1u);
+          umma_bf16(tmem, dah, dbh, idesc, 1u);
+        }
+        umma_commit(&sm.empty[s]);
       }
-      umma_commit(&sm.empty[s]);
+      // completion of every MMA issued above (also on the error path, before TMEM is released)
+      umma_commit(&sm.accfull);
     }
-    // completion of every MMA issued above (also on the error path, before TMEM is released)
-    umma_commit(&sm.accfull);
-  }
-
-  // ---- epilogue (warps 0-3: TMEM lane quarter = warp): accumulator -> FP64 output blocks
-  if (warp < 4) {
-    bool have = nchunk > 0 && mbar_wait(&sm.accfull, 0, P.err, &sm.abort, 2000000000ull);
+  } else {
+    // ---- epilogue (warps 0-3, TMEM lane quarter = warp): accumulator -> FP64 output blocks
+    bool have = nstage > 0 && mbar_wait(&sm.accfull, 0, P.err, &sm.abort, 2000000000ull);
     have = __all_sync(0xffffffffu, have && !*(volatile int*)&sm.abort);   // tcgen05.ld is warp-wide
     tc_fence_after();
     const int m = warp * 32 + lane;
@@ -401,13 +344,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_mult_umma(UmmaArgs P) {
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == kProducerWarps) {
+  if (warp == 5) {
     tc_fence_after();
-    // after an aborted pipeline the epilogue may not have seen the MMAs complete: wait for them (bounded)
-    // before the tensor memory is released
-    if (nchunk > 0 && *(volatile int*)&sm.abort) {
+    // after an aborted pipeline the epilogue may not have seen the copies and MMAs complete: wait for
+    // them (bounded) before the tensor memory and the shared memory are released
+    if (nstage > 0 && *(volatile int*)&sm.abort) {
       int dummy = 0;
-      mbar_wait(&sm.accfull, 0, P.err, &dummy, 2000000000ull);
+      if (lane == 0) mbar_wait(&sm.accfull, 0, P.err, &dummy, 2000000000ull);
       __syncwarp();
     }
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
@@ -419,72 +362,98 @@ __global__ void __launch_bounds__(kThreads, 2) k_mult_umma(UmmaArgs P) {
 // ---------------------------------------------------------------------------
 namespace {
 
-// one warp per output block: mark the contraction atoms its pairs use in the tile's bit set
-__global__ void k_umma_mark(int n_out, const int64_t* __restrict__ ptr, const int2* __restrict__ pairs,
-                            const int2* __restrict__ q_tile, const int* __restrict__ xh,
-                            const int64_t* __restrict__ mark_off, unsigned int* __restrict__ mark) {
+struct PlanDev {                     // per output block / pair lookups of the plan kernels
+  const int64_t* ptr;
+  const int2* pairs;
+  const int2* q_tile;                // output block -> (tile, ii | jj << 16)
+  const int* xh;                     // X block -> candidate position of its unit in the row group
+  const int* xcov;                   // X block -> contraction atom (cover)
+  const int* ocov;                   // output block -> column atom (cover)
+  const int* unit_of;                // cover atom -> unit
+  const int* unit_pos;               // cover atom -> position in its unit
+  const int* chunk_of;               // cover atom -> column chunk
+  const int* chunk_pos;              // cover atom -> position in its chunk
+  const int64_t* mark_off;           // tile -> first bit of its candidate bit set
+  int n_chunks;
+};
+
+// one warp per output block: mark the units its pairs contract over (tile bit sets) and the
+// (unit, column chunk) B slabs they need
+__global__ void k_umma_mark(int n_out, PlanDev D, unsigned int* __restrict__ mark, unsigned int* __restrict__ bmark) {
   const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (q >= n_out) return;
-  const int t = q_tile[q].x;
-  const int64_t mo = mark_off[t];
-  for (int64_t p = ptr[q] + lane; p < ptr[q + 1]; p += 32) {
-    const int64_t bit = mo + xh[pairs[p].x];
+  const int t = D.q_tile[q].x;
+  const int64_t mo = D.mark_off[t];
+  const int ch = D.chunk_of[D.ocov[q]];
+  for (int64_t p = D.ptr[q] + lane; p < D.ptr[q + 1]; p += 32) {
+    const int x = D.pairs[p].x;
+    const int64_t bit = mo + D.xh[x];
     atomicOr(mark + (bit >> 5), 1u << (bit & 31));
+    const int64_t bk = (int64_t)D.unit_of[D.xcov[x]] * D.n_chunks + ch;
+    atomicOr(bmark + (bk >> 5), 1u << (bk & 31));
   }
 }
 
-// one thread per tile: contraction atom list, their K offsets and the tile's K extent; per-word prefix counts
-__global__ void k_umma_clist(int n_tiles, UmmaTile* __restrict__ tiles, const int64_t* __restrict__ mark_off,
+// per-word population counts of a bit set (scanned on the host afterwards)
+__global__ void k_word_count(int64_t n_words, const unsigned int* __restrict__ bits, int* __restrict__ cnt) {
+  const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < n_words) cnt[w] = __popc(bits[w]);
+}
+
+__device__ __forceinline__ int rank_of(const unsigned int* bits, const int* pre, int64_t bit) {
+  const int64_t w = bit >> 5;
+  return pre[w] + __popc(bits[w] & ((1u << (bit & 31)) - 1u));
+}
+
+// one thread per tile: without `units` its unit count, with it the unit entries (X slab, B slab)
+__global__ void k_umma_units(int n_tiles, UmmaTile* __restrict__ tiles, const int64_t* __restrict__ mark_off,
                              const int* __restrict__ mark_bits, const unsigned int* __restrict__ mark,
-                             const int* __restrict__ u_atoms, const int64_t* __restrict__ u_off,
-                             const int* __restrict__ tile_group, const int* __restrict__ cover_nsf,
-                             int* __restrict__ wpre, int* __restrict__ c_atoms, int* __restrict__ c_koff) {
+                             const int* __restrict__ u_cand, const int64_t* __restrict__ u_off,
+                             const int* __restrict__ tile_group, const int* __restrict__ tile_chunk, int n_chunks,
+                             const unsigned int* __restrict__ bmark, const int* __restrict__ bpre,
+                             int2* __restrict__ units) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n_tiles) return;
   UmmaTile& T = tiles[t];
   const int64_t w0 = mark_off[t] >> 5;
   const int nw = (mark_bits[t] + 31) >> 5;
-  const int* U = u_atoms + u_off[tile_group[t]];
-  int cnt = 0, k = 0;
+  const int g = tile_group[t];
+  const int* U = u_cand + u_off[g];
+  int cnt = 0;
   for (int w = 0; w < nw; ++w) {
-    wpre[w0 + w] = cnt;
     unsigned int m = mark[w0 + w];
     while (m) {
       const int b = __ffs(m) - 1;
       m &= m - 1;
-      if (c_atoms) {
-        const int atom = U[32 * w + b];
-        c_atoms[T.c_off + cnt] = atom;
-        c_koff[T.c_off + cnt] = k;
-        k += cover_nsf[atom];
+      if (units) {
+        const int h = 32 * w + b;
+        const int64_t bk = (int64_t)U[h] * n_chunks + tile_chunk[t];
+        units[T.u_off + cnt] = make_int2((int)(u_off[g] + h), rank_of(bmark, bpre, bk));
       }
       ++cnt;
     }
   }
-  if (c_atoms) T.k_total = k;
-  else T.n_c = cnt;
+  if (!units) T.n_u = cnt;
 }
 
-// one warp per output block: panel entries of its pairs
-__global__ void k_umma_scatter(int n_out, const int64_t* __restrict__ ptr, const int2* __restrict__ pairs,
-                               const int2* __restrict__ q_tile, const int* __restrict__ xh,
-                               const int64_t* __restrict__ mark_off, const unsigned int* __restrict__ mark,
-                               const int* __restrict__ wpre, const UmmaTile* __restrict__ tiles,
-                               const int64_t* __restrict__ x_elem, const int64_t* __restrict__ b_elem,
-                               long long* __restrict__ xpanel, long long* __restrict__ bpanel) {
+// one warp per output block: block tables of the X and B slabs from the pairs
+__global__ void k_umma_btab(int n_out, PlanDev D, const unsigned int* __restrict__ bmark, const int* __restrict__ bpre,
+                            const int64_t* __restrict__ xs_of_tile, int* __restrict__ xtab, int* __restrict__ btab) {
   const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (q >= n_out) return;
-  const int2 tq = q_tile[q];
-  const int t = tq.x, ii = tq.y & 0xffff, jj = tq.y >> 16;
-  const UmmaTile& T = tiles[t];
-  const int64_t mo = mark_off[t];
-  for (int64_t p = ptr[q] + lane; p < ptr[q + 1]; p += 32) {
-    const int2 pr = pairs[p];
-    const int64_t bit = mo + xh[pr.x];
-    const int64_t w = bit >> 5;
-    const int pos = wpre[w] + __popc(mark[w] & ((1u << (bit & 31)) - 1u));
-    xpanel[T.xp_off + (int64_t)pos * T.n_rows + ii] = x_elem[pr.x];
-    bpanel[T.bp_off + (int64_t)pos * T.n_cols + jj] = b_elem[pr.y];
+  const int2 tq = D.q_tile[q];
+  const int ii = tq.y & 0xffff;
+  const int oc = D.ocov[q];
+  const int ch = D.chunk_of[oc], jpos = D.chunk_pos[oc];
+  const int64_t uo = xs_of_tile[tq.x];
+  for (int64_t p = D.ptr[q] + lane; p < D.ptr[q + 1]; p += 32) {
+    const int2 pr = D.pairs[p];
+    const int c = D.xcov[pr.x];
+    const int cpos = D.unit_pos[c];
+    const int64_t xs = uo + D.xh[pr.x];
+    xtab[xs * (kMaxUnitAtoms * kMaxAtoms) + cpos * kMaxAtoms + ii] = pr.x;
+    const int bs = rank_of(bmark, bpre, (int64_t)D.unit_of[c] * D.n_chunks + ch);
+    btab[(int64_t)bs * (kMaxUnitAtoms * kMaxAtoms) + cpos * kMaxAtoms + jpos] = pr.y;
   }
 }
 
@@ -503,139 +472,207 @@ UmmaPlan& get_umma_plan(System& S, int mult_type, int ra, int rb, int rc) {
   RangeIndex& O = mult_type == 1 ? *S.ranges[rc] : *S.ranges[ra];
   RangeIndex& X = mult_type == 1 ? *S.ranges[ra] : *S.ranges[rc];
   const Geometry& g = S.geo;
-  const int np = g.n_prim;
+  const int np = g.n_prim, ncov = g.n_cover_atoms;
   std::vector<int> nd_prim(np);
   for (int p = 0; p < np; ++p) nd_prim[p] = g.nsf[g.prim_global[p]];
   U.usable = true;
-  for (int p = 0; p < np; ++p) U.usable = U.usable && nd_prim[p] >= kMinNd && nd_prim[p] <= kM;
-  for (int c = 0; c < g.n_cover_atoms; ++c) U.usable = U.usable && g.cover_nsf[c] >= kMinNd && g.cover_nsf[c] <= kNT;
+  for (int p = 0; p < np; ++p) U.usable = U.usable && nd_prim[p] >= kMinNd && nd_prim[p] <= kUK;
+  for (int c = 0; c < ncov; ++c) U.usable = U.usable && g.cover_nsf[c] >= kMinNd && g.cover_nsf[c] <= kUK;
   if (!U.usable || O.nnz == 0) {
     auto res = S.uplans.emplace(key, std::move(up));
     return *res.first->second;
   }
+  // contraction units and column chunks over the cover atoms (cover order, the same for every row group)
+  std::vector<int> unit_of(ncov), unit_pos(ncov), chunk_of(ncov), chunk_pos(ncov), chunk_first;
+  std::vector<unsigned int> ktab;                   // [unit][16]
+  {
+    int u = -1, uw = kUK + 1, ua = kMaxUnitAtoms;
+    for (int c = 0; c < ncov; ++c) {
+      const int nd = g.cover_nsf[c];
+      if (uw + nd > kUK || ua == kMaxUnitAtoms) { ++u; uw = 0; ua = 0; ktab.resize((size_t)(u + 1) * kUK, 0xffffffffu); }
+      for (int o = 0; o < nd; ++o) ktab[(size_t)u * kUK + uw + o] = (unsigned)ua | ((unsigned)o << 8) | ((unsigned)nd << 16);
+      unit_of[c] = u; unit_pos[c] = ua;
+      uw += nd; ++ua;
+    }
+    int w = kNT + 1, cnt = kMaxAtoms;
+    for (int c = 0; c < ncov; ++c) {
+      const int nd = g.cover_nsf[c];
+      if (w + nd > kNT || cnt == kMaxAtoms) { chunk_first.push_back(c); w = 0; cnt = 0; }
+      chunk_of[c] = (int)chunk_first.size() - 1;
+      chunk_pos[c] = cnt;
+      w += nd; ++cnt;
+    }
+    chunk_first.push_back(ncov);
+  }
+  const int n_units = (int)(ktab.size() / kUK), n_chunks = (int)chunk_first.size() - 1;
   // host copies of the output and first-operand neighbour lists
   std::vector<int> ocov(O.nnz), xcov(std::max(X.nnz, 1));
   CQ_CUDA(cudaMemcpyAsync(ocov.data(), O.nb_cover.p, sizeof(int) * O.nnz, cudaMemcpyDeviceToHost, st));
   if (X.nnz) CQ_CUDA(cudaMemcpyAsync(xcov.data(), X.nb_cover.p, sizeof(int) * X.nnz, cudaMemcpyDeviceToHost, st));
   CQ_CUDA(cudaStreamSynchronize(st));
-  // row groups: consecutive primary atoms, at most kM rows
+  // row groups: consecutive primary atoms, at most kM rows and kMaxAtoms atoms
   std::vector<int> grp_first;
-  for (int p = 0, rows = kM + 1; p < np; ++p) {
-    if (rows + nd_prim[p] > kM) { grp_first.push_back(p); rows = 0; }
-    rows += nd_prim[p];
+  for (int p = 0, rows = kM + 1, cnt = 0; p < np; ++p) {
+    if (rows + nd_prim[p] > kM || cnt == kMaxAtoms) { grp_first.push_back(p); rows = 0; cnt = 0; }
+    rows += nd_prim[p]; ++cnt;
   }
   grp_first.push_back(np);
   const int ng = (int)grp_first.size() - 1;
+  // row tables of the row groups (offset 128 g) and of the column chunks (offset 128 (ng + chunk))
+  std::vector<unsigned int> rtabs((size_t)(ng + n_chunks) * kM, 0xffffffffu);
+  for (int gi = 0; gi < ng; ++gi)
+    for (int p = grp_first[gi], off = 0; p < grp_first[gi + 1]; off += nd_prim[p], ++p)
+      for (int o = 0; o < nd_prim[p]; ++o)
+        rtabs[(size_t)gi * kM + off + o] = (unsigned)(p - grp_first[gi]) | ((unsigned)o << 8) | ((unsigned)nd_prim[p] << 16);
+  for (int ch = 0; ch < n_chunks; ++ch)
+    for (int c = chunk_first[ch], off = 0; c < chunk_first[ch + 1]; off += g.cover_nsf[c], ++c)
+      for (int o = 0; o < g.cover_nsf[c]; ++o)
+        rtabs[(size_t)(ng + ch) * kM + off + o] = (unsigned)(c - chunk_first[ch]) | ((unsigned)o << 8) |
+                                                  ((unsigned)g.cover_nsf[c] << 16);
+  // tiles: (row group, column chunk) pairs holding output blocks; candidate units of each row group
   std::vector<UmmaTile> tiles;
-  std::vector<int> col_atoms, outmap, tile_group, mark_bits;
+  std::vector<int> outmap, tile_group, tile_chunk, mark_bits, u_cand, xh(std::max(X.nnz, 1), 0);
   std::vector<int2> q_tile(O.nnz);
-  std::vector<int> xh(std::max(X.nnz, 1), 0);
-  std::vector<int> u_atoms;
   std::vector<int64_t> u_off(ng + 1, 0), mark_off;
   int64_t mark_total = 0;
   for (int gi = 0; gi < ng; ++gi) {
     const int r0 = grp_first[gi], r1 = grp_first[gi + 1];
-    // output columns of the group: sorted cover atoms of its rows, cut into runs of <= kNT orbitals
-    std::vector<int> cols(ocov.begin() + O.h_row_ptr[r0], ocov.begin() + O.h_row_ptr[r1]);
-    std::sort(cols.begin(), cols.end());
-    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
-    std::vector<int> chunk_of(cols.size()), pos_in(cols.size());
-    std::vector<int> chunk_first;
-    for (size_t c = 0, w = kNT + 1, cnt = kMaxRowAtoms; c < cols.size(); ++c) {
-      const int nd = g.cover_nsf[cols[c]];
-      if (w + nd > (size_t)kNT || cnt == (size_t)kMaxRowAtoms) { chunk_first.push_back((int)c); w = 0; cnt = 0; }
-      chunk_of[c] = (int)chunk_first.size() - 1;
-      pos_in[c] = (int)(c - chunk_first.back());
-      w += nd; ++cnt;
-    }
-    chunk_first.push_back((int)cols.size());
-    // contraction candidates of the group: sorted cover atoms of the first operand's rows
-    std::vector<int> cand(xcov.begin() + X.h_row_ptr[r0], xcov.begin() + X.h_row_ptr[r1]);
+    std::vector<int> chs;
+    for (int q = O.h_row_ptr[r0]; q < O.h_row_ptr[r1]; ++q) chs.push_back(chunk_of[ocov[q]]);
+    std::sort(chs.begin(), chs.end());
+    chs.erase(std::unique(chs.begin(), chs.end()), chs.end());
+    std::vector<int> cand;
+    for (int e = X.h_row_ptr[r0]; e < X.h_row_ptr[r1]; ++e) cand.push_back(unit_of[xcov[e]]);
     std::sort(cand.begin(), cand.end());
     cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
     for (int e = X.h_row_ptr[r0]; e < X.h_row_ptr[r1]; ++e)
-      xh[e] = (int)(std::lower_bound(cand.begin(), cand.end(), xcov[e]) - cand.begin());
-    u_off[gi] = (int64_t)u_atoms.size();
-    u_atoms.insert(u_atoms.end(), cand.begin(), cand.end());
+      xh[e] = (int)(std::lower_bound(cand.begin(), cand.end(), unit_of[xcov[e]]) - cand.begin());
+    u_off[gi] = (int64_t)u_cand.size();
+    u_cand.insert(u_cand.end(), cand.begin(), cand.end());
     const int t0 = (int)tiles.size();
-    for (size_t ch = 0; ch + 1 < chunk_first.size(); ++ch) {
+    for (int ch : chs) {
       UmmaTile T{};
       T.row_first = r0;
       T.n_rows = r1 - r0;
-      T.col_off = (int)col_atoms.size();
       T.n_cols = chunk_first[ch + 1] - chunk_first[ch];
+      T.row_tab = gi * kM;
+      T.col_tab = (ng + ch) * kM;
       T.om_off = (int)outmap.size();
-      for (int c = chunk_first[ch]; c < chunk_first[ch + 1]; ++c) col_atoms.push_back(cols[c]);
       outmap.resize(outmap.size() + (size_t)T.n_rows * T.n_cols, -1);
       tiles.push_back(T);
       tile_group.push_back(gi);
+      tile_chunk.push_back(ch);
       mark_off.push_back(mark_total);
       mark_bits.push_back((int)cand.size());
       mark_total += ((int64_t)cand.size() + 31) / 32 * 32;
     }
     for (int p = r0; p < r1; ++p)
       for (int q = O.h_row_ptr[p]; q < O.h_row_ptr[p + 1]; ++q) {
-        const int c = (int)(std::lower_bound(cols.begin(), cols.end(), ocov[q]) - cols.begin());
-        const int t = t0 + chunk_of[c];
-        const int ii = p - r0, jj = pos_in[c];
+        const int ch = chunk_of[ocov[q]];
+        const int t = t0 + (int)(std::lower_bound(chs.begin(), chs.end(), ch) - chs.begin());
+        const int ii = p - r0, jj = chunk_pos[ocov[q]];
         q_tile[q] = make_int2(t, ii | (jj << 16));
         outmap[tiles[t].om_off + ii * tiles[t].n_cols + jj] = q;
       }
   }
-  u_off[ng] = (int64_t)u_atoms.size();
+  u_off[ng] = (int64_t)u_cand.size();
   const int nt = (int)tiles.size();
   U.n_tiles = nt;
+  U.n_xslabs = u_off[ng];
+  std::vector<int64_t> xs_tile(nt);
+  for (int t = 0; t < nt; ++t) xs_tile[t] = u_off[tile_group[t]];
+  // device copies of the plan inputs
   DevBuf<int2> d_qt; d_qt.upload(q_tile, st);
   DevBuf<int> d_xh; d_xh.upload(xh, st);
+  DevBuf<int> d_xcov; d_xcov.upload(xcov, st);
+  DevBuf<int> d_uof; d_uof.upload(unit_of, st);
+  DevBuf<int> d_upos; d_upos.upload(unit_pos, st);
+  DevBuf<int> d_chof; d_chof.upload(chunk_of, st);
+  DevBuf<int> d_chpos; d_chpos.upload(chunk_pos, st);
   DevBuf<int64_t> d_moff; d_moff.upload(mark_off, st);
   DevBuf<int> d_mbits; d_mbits.upload(mark_bits, st);
   DevBuf<int> d_tg; d_tg.upload(tile_group, st);
-  DevBuf<int> d_u; d_u.upload(u_atoms.empty() ? std::vector<int>{0} : u_atoms, st);
+  DevBuf<int> d_tc; d_tc.upload(tile_chunk, st);
+  DevBuf<int> d_uc; d_uc.upload(u_cand.empty() ? std::vector<int>{0} : u_cand, st);
   DevBuf<int64_t> d_uoff; d_uoff.upload(u_off, st);
-  DevBuf<unsigned int> d_mark; d_mark.alloc(std::max<int64_t>(mark_total / 32, 1), st);
-  CQ_CUDA(cudaMemsetAsync(d_mark.p, 0, sizeof(unsigned int) * d_mark.n, st));
-  DevBuf<int> d_wpre; d_wpre.alloc(d_mark.n, st);
+  DevBuf<int64_t> d_xst; d_xst.upload(xs_tile, st);
+  const int64_t mark_words = std::max<int64_t>(mark_total / 32, 1);
+  const int64_t bkeys = (int64_t)n_units * n_chunks;
+  const int64_t bwords = std::max<int64_t>((bkeys + 31) / 32, 1);
+  DevBuf<unsigned int> d_mark; d_mark.alloc(mark_words, st);
+  DevBuf<unsigned int> d_bmark; d_bmark.alloc(bwords, st);
+  CQ_CUDA(cudaMemsetAsync(d_mark.p, 0, sizeof(unsigned int) * mark_words, st));
+  CQ_CUDA(cudaMemsetAsync(d_bmark.p, 0, sizeof(unsigned int) * bwords, st));
   U.tiles.upload(tiles, st);
-  U.col_atoms.upload(col_atoms.empty() ? std::vector<int>{0} : col_atoms, st);
   U.outmap.upload(outmap.empty() ? std::vector<int>{-1} : outmap, st);
-  const int T256 = 256;
+  U.rtabs.upload(rtabs, st);
+  U.ktabs.upload(ktab, st);
+  PlanDev D;
+  D.ptr = P.ptr.p; D.pairs = P.pairs.p; D.q_tile = d_qt.p; D.xh = d_xh.p; D.xcov = d_xcov.p; D.ocov = O.nb_cover.p;
+  D.unit_of = d_uof.p; D.unit_pos = d_upos.p; D.chunk_of = d_chof.p; D.chunk_pos = d_chpos.p; D.mark_off = d_moff.p;
+  D.n_chunks = n_chunks;
   const int n_out = O.nnz;
-  k_umma_mark<<<(int)(((int64_t)n_out * 32 + T256 - 1) / T256), T256, 0, st>>>(n_out, P.ptr.p, P.pairs.p, d_qt.p, d_xh.p,
-                                                                               d_moff.p, d_mark.p);
-  k_umma_clist<<<(nt + 127) / 128, 128, 0, st>>>(nt, U.tiles.p, d_moff.p, d_mbits.p, d_mark.p, d_u.p, d_uoff.p, d_tg.p,
-                                                 S.dg.cover_nsf.p, d_wpre.p, nullptr, nullptr);
+  const int T256 = 256;
+  const int gw = (int)(((int64_t)n_out * 32 + T256 - 1) / T256);
+  k_umma_mark<<<gw, T256, 0, st>>>(n_out, D, d_mark.p, d_bmark.p);
+  k_umma_units<<<(nt + 127) / 128, 128, 0, st>>>(nt, U.tiles.p, d_moff.p, d_mbits.p, d_mark.p, d_uc.p, d_uoff.p, d_tg.p,
+                                                 d_tc.p, n_chunks, d_bmark.p, nullptr, nullptr);
+  // ranks of the B slab keys: per-word counts, scanned on the host
+  DevBuf<int> d_bpre; d_bpre.alloc(bwords, st);
+  k_word_count<<<(int)((bwords + 255) / 256), 256, 0, st>>>(bwords, d_bmark.p, d_bpre.p);
   CQ_CUDA(cudaGetLastError());
-  // sizes of the contraction lists and panels
+  std::vector<int> bpre(bwords);
+  std::vector<unsigned int> bm(bwords);
+  CQ_CUDA(cudaMemcpyAsync(bpre.data(), d_bpre.p, sizeof(int) * bwords, cudaMemcpyDeviceToHost, st));
+  CQ_CUDA(cudaMemcpyAsync(bm.data(), d_bmark.p, sizeof(unsigned int) * bwords, cudaMemcpyDeviceToHost, st));
   CQ_CUDA(cudaMemcpyAsync(tiles.data(), U.tiles.p, sizeof(UmmaTile) * nt, cudaMemcpyDeviceToHost, st));
   CQ_CUDA(cudaStreamSynchronize(st));
-  int64_t coff = 0, xoff = 0, boff = 0;
-  for (auto& T : tiles) {
-    T.c_off = (int)coff;
-    T.xp_off = xoff;
-    T.bp_off = boff;
-    coff += T.n_c;
-    xoff += (int64_t)T.n_c * T.n_rows;
-    boff += (int64_t)T.n_c * T.n_cols;
-  }
-  CQ_CHECK(coff < (int64_t)1 << 31, CQ_ERR_BOUNDS, "tensor-core tile plan: contraction list too long");
-  U.tiles.upload(tiles, st);
-  U.c_atoms.alloc(std::max<int64_t>(coff, 1), st);
-  U.c_koff.alloc(std::max<int64_t>(coff, 1), st);
-  U.xpanel.alloc(std::max<int64_t>(xoff, 1), st);
-  U.bpanel.alloc(std::max<int64_t>(boff, 1), st);
-  CQ_CUDA(cudaMemsetAsync(U.xpanel.p, 0xff, sizeof(long long) * U.xpanel.n, st));
-  CQ_CUDA(cudaMemsetAsync(U.bpanel.p, 0xff, sizeof(long long) * U.bpanel.n, st));
-  k_umma_clist<<<(nt + 127) / 128, 128, 0, st>>>(nt, U.tiles.p, d_moff.p, d_mbits.p, d_mark.p, d_u.p, d_uoff.p, d_tg.p,
-                                                 S.dg.cover_nsf.p, d_wpre.p, U.c_atoms.p, U.c_koff.p);
-  k_umma_scatter<<<(int)(((int64_t)n_out * 32 + T256 - 1) / T256), T256, 0, st>>>(
-      n_out, P.ptr.p, P.pairs.p, d_qt.p, d_xh.p, d_moff.p, d_mark.p, d_wpre.p, U.tiles.p, X.nb_elem.p,
-      S.ranges[rb]->nb_elem.p, U.xpanel.p, U.bpanel.p);
-  CQ_CUDA(cudaGetLastError());
-  CQ_CUDA(cudaMemcpyAsync(tiles.data(), U.tiles.p, sizeof(UmmaTile) * nt, cudaMemcpyDeviceToHost, st));
-  CQ_CUDA(cudaStreamSynchronize(st));
+  int64_t n_bslabs = 0;
+  for (auto& x : bpre) { const int c = x; x = (int)n_bslabs; n_bslabs += c; }
+  d_bpre.upload(bpre, st);
+  U.n_bslabs = n_bslabs;
+  int64_t uoff = 0;
   U.issued_flops = 0;
-  for (auto& T : tiles) U.issued_flops += 3ll * 2 * kM * kNT * (((int64_t)T.k_total + kKC - 1) / kKC * kKC);
-  S.launches += 3;
+  for (auto& T : tiles) {
+    T.u_off = (int)uoff;
+    uoff += T.n_u;
+    U.issued_flops += 3ll * 2 * kM * kNT * kUK * T.n_u;
+  }
+  CQ_CHECK(uoff < ((int64_t)1 << 31) && n_bslabs < ((int64_t)1 << 31) && U.n_xslabs < ((int64_t)1 << 31), CQ_ERR_BOUNDS,
+           "tensor-core tile plan too large");
+  U.tiles.upload(tiles, st);
+  U.units.alloc(std::max<int64_t>(uoff, 1), st);
+  k_umma_units<<<(nt + 127) / 128, 128, 0, st>>>(nt, U.tiles.p, d_moff.p, d_mbits.p, d_mark.p, d_uc.p, d_uoff.p, d_tg.p,
+                                                 d_tc.p, n_chunks, d_bmark.p, d_bpre.p, U.units.p);
+  // block tables of the slabs, and the per-slab row tables / units of the packing kernels
+  const int64_t tabw = kMaxUnitAtoms * kMaxAtoms;
+  U.xtab.alloc(std::max<int64_t>(U.n_xslabs, 1) * tabw, st);
+  U.btab.alloc(std::max<int64_t>(n_bslabs, 1) * tabw, st);
+  CQ_CUDA(cudaMemsetAsync(U.xtab.p, 0xff, sizeof(int) * U.xtab.n, st));
+  CQ_CUDA(cudaMemsetAsync(U.btab.p, 0xff, sizeof(int) * U.btab.n, st));
+  k_umma_btab<<<gw, T256, 0, st>>>(n_out, D, d_bmark.p, d_bpre.p, d_xst.p, U.xtab.p, U.btab.p);
+  CQ_CUDA(cudaGetLastError());
+  std::vector<int> xs_rtab(std::max<int64_t>(U.n_xslabs, 1), 0), xs_unit(std::max<int64_t>(U.n_xslabs, 1), 0);
+  for (int gi = 0; gi < ng; ++gi)
+    for (int64_t h = u_off[gi]; h < u_off[gi + 1]; ++h) { xs_rtab[h] = gi * kM; xs_unit[h] = u_cand[h]; }
+  U.xs_rtab.upload(xs_rtab, st);
+  U.xs_unit.upload(xs_unit, st);
+  // B slabs in key order (key = unit * n_chunks + chunk), as ranked above
+  std::vector<int> bs_rtab, bs_unit;
+  bs_rtab.reserve(std::max<int64_t>(n_bslabs, 1)); bs_unit.reserve(std::max<int64_t>(n_bslabs, 1));
+  for (int64_t w = 0; w < bwords; ++w)
+    for (unsigned int m = bm[w]; m; m &= m - 1) {
+      const int64_t k = 32 * w + __builtin_ctz(m);
+      bs_unit.push_back((int)(k / n_chunks));
+      bs_rtab.push_back((int)((ng + k % n_chunks) * kM));
+    }
+  if (bs_rtab.empty()) { bs_rtab.push_back(0); bs_unit.push_back(0); }
+  U.bs_rtab.upload(bs_rtab, st);
+  U.bs_unit.upload(bs_unit, st);
+  U.xslabs.alloc((size_t)std::max<int64_t>(U.n_xslabs, 1) * (kSlabBytes / 16), st);
+  U.bslabs.alloc((size_t)std::max<int64_t>(n_bslabs, 1) * (kSlabBytes / 16), st);
+  CQ_CUDA(cudaStreamSynchronize(st));
+  S.launches += 5;
   auto res = S.uplans.emplace(key, std::move(up));
   return *res.first->second;
 }
@@ -655,30 +692,43 @@ bool umma_usable(System& S, int mult_type, int ra, int rb, int rc) {
 
 void mat_mult_umma(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c) {
   UmmaPlan& U = get_umma_plan(S, mult_type, ra, rb, rc);
-  CQ_CHECK(U.usable, CQ_ERR_ARG, "tensor-core tiles need block sizes of 4 to 128");
+  CQ_CHECK(U.usable, CQ_ERR_ARG, "tensor-core tiles need block sizes of 4 to 16");
   if (U.n_tiles == 0) return;
   RangeIndex &A = *S.ranges[ra], &B = *S.ranges[rb], &C = *S.ranges[rc];
   RangeIndex& O = mult_type == 1 ? C : A;
+  RangeIndex& X = mult_type == 1 ? A : C;
+  cudaStream_t st = S.stream;
+  cudaEvent_t ev0 = nullptr;
+  if (S.prof.on) { ev0 = S.prof.get(); CQ_CUDA(cudaEventRecord(ev0, st)); }
+  // pack the operands: X slabs (first operand, row orbital fastest), B slabs (type 1: B(k, j) with the
+  // K orbital fastest; type 2: B(k, j) with the column orbital fastest)
+  PackArgs pk;
+  pk.ktabs = U.ktabs.p;
+  pk.rtabs = U.rtabs.p;
+  if (U.n_xslabs > 0) {
+    pk.slab_rtab = U.xs_rtab.p; pk.slab_unit = U.xs_unit.p; pk.btab = U.xtab.p;
+    pk.elem = X.nb_elem.p; pk.src = mult_type == 1 ? a : c; pk.out = U.xslabs.p; pk.k_fastest = 0;
+    k_umma_pack<<<(int)U.n_xslabs, 256, 0, st>>>(pk);
+  }
+  if (U.n_bslabs > 0) {
+    pk.slab_rtab = U.bs_rtab.p; pk.slab_unit = U.bs_unit.p; pk.btab = U.btab.p;
+    pk.elem = B.nb_elem.p; pk.src = b; pk.out = U.bslabs.p; pk.k_fastest = mult_type == 1 ? 1 : 0;
+    k_umma_pack<<<(int)U.n_bslabs, 256, 0, st>>>(pk);
+  }
   UmmaArgs M;
-  M.tiles = U.tiles.p; M.col_atoms = U.col_atoms.p; M.c_atoms = U.c_atoms.p; M.c_koff = U.c_koff.p;
-  M.xpanel = U.xpanel.p; M.bpanel = U.bpanel.p; M.outmap = U.outmap.p;
-  M.prim_nsf = S.dg.prim_nsf.p; M.cover_nsf = S.dg.cover_nsf.p;
+  M.tiles = U.tiles.p; M.units = U.units.p; M.rtabs = U.rtabs.p; M.outmap = U.outmap.p;
+  M.xslabs = U.xslabs.p; M.bslabs = U.bslabs.p;
   M.o_elem = O.nb_elem.p;
-  M.x = mult_type == 1 ? a : c;
-  M.b = b;
   M.out = mult_type == 1 ? c : a;
-  M.type = mult_type;
   M.err = umma_err_word(S);
   const size_t smem = sizeof(Smem) + 1024;
   CQ_CUDA(cudaFuncSetAttribute(k_mult_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  cudaEvent_t ev0 = nullptr;
-  if (S.prof.on) { ev0 = S.prof.get(); CQ_CUDA(cudaEventRecord(ev0, S.stream)); }
-  k_mult_umma<<<U.n_tiles, kThreads, smem, S.stream>>>(M);
+  k_mult_umma<<<U.n_tiles, kThreads, smem, st>>>(M);
   CQ_CUDA(cudaGetLastError());
-  S.launches++;
+  S.launches += 3;
   if (S.prof.on) {
     cudaEvent_t ev1 = S.prof.get();
-    CQ_CUDA(cudaEventRecord(ev1, S.stream));
+    CQ_CUDA(cudaEventRecord(ev1, st));
     S.prof.recs.push_back({ev0, ev1, 8.0 * (double)(A.length + B.length + C.length), (double)U.flops});
   }
 }
