@@ -211,6 +211,54 @@ def cpu_record():
     return json.load(open(p)) if os.path.exists(p) else None
 
 
+def cpu_full_solve(path):
+    """One complete solve of the workload on the CPU chain (T = S^-1, McWeeny start, FindMinDM to
+    convergence), the oracle's restatement with the ompGemm kernel on every host core, timed end to end."""
+    from cq_b200 import inputs
+    import cq_b200
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from cq_oracle import OracleSystem
+    from lnv_oracle import OracleLNV, Params
+    coords, cell = inputs.diamond_si(CFG["ncell"], sigma=CFG["sigma"], seed=CFG["seed"])
+    n = len(coords)
+    rng = cq_b200.lnv_ranges(CFG["rs"], CFG["rh"], CFG["rl"], CFG["rt"])
+    ridx = {k: i for i, k in enumerate(rng)}
+    o = OracleSystem(coords, cell, np.full(n, CFG["nsf"]), list(rng.values()))
+    S = inputs.overlap_S(o.blocklist(ridx["S"], coords, cell))
+    H = inputs.hamiltonian_H(o.blocklist(ridx["H"], coords, cell), seed=CFG["h_seed"])
+    nth = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(nth)
+    lnv = OracleLNV(o, ridx, S, H, CFG["ne_per_atom"] * n / 2.0, float(CFG["nsf"] * n), Params(), kernel="ompGemm",
+                    nthreads=nth)
+    t0 = time.perf_counter()
+    lnv.iter_hott_invs()
+    E, N = lnv.find_min_dm()
+    t = time.perf_counter() - t0
+    rec = {"workload": WORKLOAD, "what": "one complete solve on the CPU chain (oracle restatement, ompGemm kernel, "
+                                         "OpenBLAS dgemm with one thread per OpenMP thread)",
+           "cores": nth, "seconds": t, "energy": E, "electrons": N, "products": int(lnv.n_products),
+           "flops": int(lnv.flops), "converged": bool(lnv.converged),
+           "command": "python bench.py --cpu-full-solve " + os.path.relpath(path, ROOT)}
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    json.dump(rec, open(path, "w"), indent=1)
+    emit(rec)
+
+
+def fixture_parity(res):
+    """The timed solve against the oracle chain's committed fixture of this workload
+    (tests/golden/lnv_chain_si512.json): energy, electron count and product count."""
+    p = os.path.join(ROOT, "tests", "golden", "lnv_chain_si512.json")
+    if not os.path.exists(p):
+        return None
+    gold = json.load(open(p))["cases"]["r10_12_16_10"]
+    return {"fixture": "tests/golden/lnv_chain_si512.json", "oracle_energy": gold["energy"],
+            "oracle_electrons": gold["electrons"], "oracle_products": gold["n_products"],
+            "energy_identical": res["energy"] == gold["energy"],
+            "energy_rel_diff": abs(res["energy"] - gold["energy"]) / abs(gold["energy"]),
+            "electrons_rel_diff": abs(res["electrons"] - gold["electrons"]) / abs(gold["electrons"]),
+            "products_identical": res["n_products"] == gold["n_products"]}
+
+
 def config_of(n, ne_spin, ws):
     return {"workload": WORKLOAD, "atoms": n, "blocks": "4x4", "ranges_bohr": {"S": 10, "H": 12, "L": 16, "T": 10},
             "electrons": int(2 * ne_spin), "n_L_iterations": 50, "tolerance": 1e-7,
@@ -310,6 +358,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed-sample", action="store_true",
+                    help="skip the mixed-precision vs FP64 comparison on the bounded DZP sample")
     ap.add_argument("--workload", default="lnv512", choices=["lnv512", "batch", "serve", "mult216", "mult512", "mult4096"],
                     help="lnv512: the plain FP64 512-atom solve (default); batch / serve: mixed-precision solves of "
                          "many systems on concurrent slots vs the FP64 path one at a time; mult216 / mult512: single "
@@ -317,10 +367,13 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3"])
     ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (-1 autotuned, 0..3, 5)")
     ap.add_argument("--mixed-kernel", type=int, default=-1, choices=[-1, 0, 1],
-                    help="split-precision products: -1 = the faster, timed per product (default), 0 = tcgen05 tiles, "
-                         "1 = one block per mma.sync warp")
+                    help="split-precision products: -1 = chosen per product by the tile plan's useful fraction "
+                         "(default), 0 = tcgen05 tiles, 1 = one block per mma.sync warp")
     ap.add_argument("--work-record", default=None,
                     help="write the workload's per-solve work (flops, products, energy) as JSON to this path")
+    ap.add_argument("--cpu-full-solve", default=None, metavar="PATH",
+                    help="time one complete solve of the workload on the CPU chain (the oracle's ompGemm restatement, "
+                         "all host cores; several minutes) and write the record as JSON to PATH")
     ap.add_argument("--one-solve", action="store_true",
                     help="run exactly one solve of the workload and print its result (for launch lists under ncu)")
     ap.add_argument("--requests", type=int, default=32)
@@ -342,6 +395,10 @@ def main():
         return
     if args.impl == "reference":
         return reference_main(args, ws, rank)
+    if args.cpu_full_solve:
+        if rank == 0:
+            cpu_full_solve(args.cpu_full_solve)
+        return
     import torch
     import cq_b200
     torch.cuda.set_device(local)
@@ -449,6 +506,10 @@ def main():
                              "%.3g flop of products" % (p_c, f_c, t_c, nth, per_solve_flops),
                    "full_solve_timed": cpu_record()}
         clocks = clk.summary()
+        mixed = None
+        if ws == 1 and not args.no_mixed_sample:
+            torch.cuda.synchronize()
+            mixed = mixed_vs_fp64(cq_b200)
         srt = sorted(steps_ms)
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
@@ -459,6 +520,8 @@ def main():
             "solve": {"energy": res["energy"], "electrons": res["electrons"], "products": res["n_products"],
                       "flops": per_solve_flops, "late_iters": res["late_iters"], "early_iters": res["early_iters"],
                       "mcw_sweeps": res["mcw_sweeps"], "converged": res["converged"]},
+            "parity": fixture_parity(res),
+            "mixed_vs_fp64": mixed,
             "block_mult_tflops": (prof["flops"] / (prof["ms"] / 1e3) / 1e12) if prof["ms"] > 0 else None,
             "roofline": {"bound": "hbm", "kernel": "FP64 4x4 block products (autotuned k_mult_nd4_warp / k_mult_nd4_quad)", "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
@@ -532,6 +595,42 @@ def run_server(cq_b200, reqs, n_slots, mixed, rate=None, seed=0):
     t1 = max(x["t_done"] for x in res)
     srv.close()
     return res, t1 - t0
+
+
+def mixed_sample_requests():
+    """Bounded DZP sample of the mixed-precision comparison in the default bench line: two Si clusters
+    (64 and 100 atoms) and two periodic supercells (64 atoms, sigma 0.1 bohr, different seeds), 13x13
+    blocks, 2 electrons per atom, ranges as the 512-atom workload, per-request generator seeds."""
+    from cq_b200 import inputs
+    out = []
+    for k, (kind, n) in enumerate((("cluster", 64), ("cell", 2), ("cluster", 100), ("cell", 2))):
+        if kind == "cluster":
+            c, cell = inputs.si_cluster(n, sigma=0.1, seed=2000 + k)
+        else:
+            c, cell = inputs.diamond_si(n, sigma=0.1, seed=2000 + k)
+        out.append(dict(coords=c, cell=cell, nsf=13, ne=2.0 * len(c), seed=6000 + k, n=len(c)))
+    return out
+
+
+def mixed_vs_fp64(cq_b200):
+    """The precision form against the plain FP64 path on the bounded DZP sample: FP64 solves one at a
+    time, mixed-precision solves on 4 concurrent slots; both stop at residual SERVE_TOL (pass limit
+    SERVE_MAX_OUTER).  Solves/s of both arms, their ratio and the largest |dE| per atom."""
+    reqs = mixed_sample_requests()
+    fp, t_fp = run_server(cq_b200, reqs, 1, False)
+    mx, t_mx = run_server(cq_b200, reqs, 4, True)
+    ok = [(a, b) for a, b in zip(fp, mx) if a["status"] == 0 and b["status"] == 0]
+    err = max([abs(a["energy"] - b["energy"]) / a["n_atoms"] for a, b in ok], default=None)
+    return {"sample": "4 DZP (13x13) Si systems: clusters of 64 and 100 atoms, two 64-atom supercells; S/H/L/T "
+                      "10/12/16/10 bohr; both arms stop at residual %g (pass limit %d)" % (SERVE_TOL, SERVE_MAX_OUTER),
+            "fp64": {"solves_per_s": len(reqs) / t_fp, "seconds": t_fp, "slots": 1},
+            "mixed": {"solves_per_s": len(reqs) / t_mx, "seconds": t_mx, "slots": 4,
+                      "precision": "bf16x3 split products (tensor cores), FP64 traces, line search, Hotelling, "
+                                   "McWeeny start and FP64 continuation from residual 1e-6"},
+            "ratio": t_fp / t_mx, "max_abs_dE_per_atom_Ha": err,
+            "converged": [int(a["converged"]) for a in fp] + [int(b["converged"]) for b in mx],
+            "failed": sum(1 for r in fp + mx if r["status"] != 0),
+            "target": "mixed >= 5x the FP64 solves/s at <= 1e-8 Ha/atom"}
 
 
 def torch_total_mem():

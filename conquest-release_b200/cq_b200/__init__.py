@@ -91,6 +91,8 @@ def lib():
         "cq_export_index": [c_void_p, c_int, ctypes.c_char_p, P(c_int64), c_int64, P(c_int64)],
         "cq_export_radius": [c_void_p, c_int, P(c_double), c_int64, P(c_int64)],
         "cq_mat_mult": [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int],
+        "cq_mat_mult_batch": [c_int, P(c_void_p), P(c_int), P(c_int), P(c_int), P(c_int), P(c_void_p), P(c_void_p),
+                              P(c_void_p), P(c_int)],
         "cq_mat_mult_host": [c_void_p, c_int, c_int, c_int, c_int, P(c_double), P(c_double), P(c_double), c_int],
         "cq_product_work": [c_void_p, c_int, c_int, c_int, c_int, P(c_int64), P(c_int64)],
         "cq_product_tuning": [c_void_p, c_int, c_int, c_int, c_int, P(c_int), P(ctypes.c_float), P(c_int),
@@ -303,8 +305,8 @@ class System:
         return t.value, f.value, bool(u.value)
 
     def set_mixed_kernel(self, k):
-        """Kernel of the split-precision products: -1 = the faster, timed per product (default), 0 = tcgen05
-        tiles, 1 = one block per mma.sync warp."""
+        """Kernel of the split-precision products: -1 = chosen per product by the tile plan's useful fraction
+        (default), 0 = tcgen05 tiles, 1 = one block per mma.sync warp."""
         check(lib().cq_system_set_option(self._h, 3, int(k)))
 
     def matrix_sum(self, ra, a, alpha, rb, b, beta):
@@ -395,6 +397,20 @@ def m_kern(kind, k_off, kpart, ib_nd_acc, ibaddr, nbnab, ibpart, ibseq, bndim2, 
     check(f(int(k_off), int(kpart), *[_ip(x) for x in arrs], _dp(a), _dp(b), _dp(c), *[_ip(x) for x in ah],
             *[_ip(x) for x in ch], int(chalo["ni_in_halo"]), *[_ip(x) for x in tr], int(mx_absb), int(mx_part),
             int(mx_iprim), a.size, b.size, c.size))
+
+
+def mat_mult_batch(products):
+    """cq_mat_mult_batch: products = [(system, mult_type, ra, rb, rc, a, b, c, precision), ...] with device
+    operands (torch CUDA tensors or integer pointers) and precision PREC_FP64 or PREC_FP64_FMA; one
+    persistent launch over all of them, bit-identical to separate mat_mult calls."""
+    n = len(products)
+    I = c_int * n
+    V = c_void_p * n
+    systems = V(*[p[0].handle.value for p in products])
+    mt, ra, rb, rc = (I(*[int(p[k]) for p in products]) for k in (1, 2, 3, 4))
+    a, b, c = (V(*[_ptr(p[k]).value for p in products]) for k in (5, 6, 7))
+    prec = I(*[int(p[8]) for p in products])
+    check(lib().cq_mat_mult_batch(n, systems, mt, ra, rb, rc, a, b, c, prec))
 
 
 def lnv_params(**kw):
@@ -533,7 +549,8 @@ def pulay_alphas(ipulay, Aij, n, max_n):
 class ServerConfig(ctypes.Structure):
     """cq_server_config (include/cq_b200.h)."""
     _fields_ = [("n_slots", c_int), ("hbm_budget", c_int64), ("max_bypass", c_int), ("blocking_sync", c_int),
-                ("dry_run", c_int), ("dry_run_seconds", c_double), ("lnv", LNVParams)]
+                ("dry_run", c_int), ("dry_run_seconds", c_double), ("lnv", LNVParams), ("batch_products", c_int),
+                ("batch_window_us", c_double)]
 
 
 class Request(ctypes.Structure):
@@ -603,12 +620,13 @@ class Server:
     """
 
     def __init__(self, n_slots=8, hbm_budget=64 << 30, max_bypass=4, blocking_sync=True, dry_run=False,
-                 dry_run_seconds=0.01, **lnv):
+                 dry_run_seconds=0.01, batch_products=False, batch_window_us=50.0, **lnv):
         L = _server_lib()
         c = ServerConfig()
         check(L.cq_server_config_default(ctypes.byref(c)))
         c.n_slots, c.hbm_budget, c.max_bypass = int(n_slots), int(hbm_budget), int(max_bypass)
         c.blocking_sync, c.dry_run, c.dry_run_seconds = int(bool(blocking_sync)), int(bool(dry_run)), float(dry_run_seconds)
+        c.batch_products, c.batch_window_us = int(bool(batch_products)), float(batch_window_us)
         for k, v in lnv.items():
             setattr(c.lnv, k, v)
         h = c_void_p()

@@ -218,6 +218,55 @@ int cq_mat_mult(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a
   });
 }
 
+int cq_mat_mult_batch(int n, cq_system* const* systems, const int* mult_type, const int* ra, const int* rb,
+                      const int* rc, double* const* a_dev, const double* const* b_dev, double* const* c_dev,
+                      const int* precision) {
+  return guarded([&] {
+    CQ_CHECK(n >= 1 && systems && mult_type && ra && rb && rc && a_dev && b_dev && c_dev && precision, CQ_ERR_ARG,
+             "null argument");
+    std::vector<BatchItem> items;
+    std::vector<cudaStream_t> streams;
+    for (int k = 0; k < n; ++k) {
+      cq_system* sys = systems[k];
+      check_sys(sys); check_range(sys, ra[k]); check_range(sys, rb[k]); check_range(sys, rc[k]);
+      CQ_CHECK(mult_type[k] == 1 || mult_type[k] == 2, CQ_ERR_ARG, "mult_type must be 1 or 2");
+      CQ_CHECK(precision[k] == CQ_PREC_FP64 || precision[k] == CQ_PREC_FP64_FMA, CQ_ERR_ARG,
+               "batched products are FP64 (CQ_PREC_FP64 or CQ_PREC_FP64_FMA)");
+      CQ_CHECK(a_dev[k] && b_dev[k] && c_dev[k], CQ_ERR_ARG, "null operand");
+      ProductPlan& P = get_plan(sys->S, mult_type[k], ra[k], rb[k], rc[k]);
+      items.push_back({&sys->S, &P, a_dev[k], b_dev[k], c_dev[k], precision[k] == CQ_PREC_FP64 ? 1 : 0});
+      if (std::find(streams.begin(), streams.end(), sys->S.stream) == streams.end()) streams.push_back(sys->S.stream);
+    }
+    // one launch on the first system's stream, after the work already on every system's stream;
+    // every system's later work waits for it
+    cudaStream_t st = streams[0];
+    std::vector<cudaEvent_t> evs;
+    auto make_event = [&] {
+      cudaEvent_t e;
+      CQ_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      evs.push_back(e);
+      return e;
+    };
+    try {
+      for (size_t k = 1; k < streams.size(); ++k) {
+        cudaEvent_t e = make_event();
+        CQ_CUDA(cudaEventRecord(e, streams[k]));
+        CQ_CUDA(cudaStreamWaitEvent(st, e, 0));
+      }
+      launch_mat_mult_batch(items, st);
+      if (streams.size() > 1) {
+        cudaEvent_t done = make_event();
+        CQ_CUDA(cudaEventRecord(done, st));
+        for (size_t k = 1; k < streams.size(); ++k) CQ_CUDA(cudaStreamWaitEvent(streams[k], done, 0));
+      }
+    } catch (...) {
+      for (cudaEvent_t e : evs) cudaEventDestroy(e);
+      throw;
+    }
+    for (cudaEvent_t e : evs) cudaEventDestroy(e);
+  });
+}
+
 int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c,
                      int exact) {
   return guarded([&] {

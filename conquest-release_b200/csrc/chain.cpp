@@ -89,6 +89,8 @@ void LNVSolver::mult_dispatch(ProductPlan& P, double* a, const double* b, double
     stats.n_products_mixed++;
     stats.flops_mixed += P.flops;
     mat_mult_mixed(S, P.mult_type, P.ra, P.rb, P.rc, a, b, c);
+  } else if (S.batch_submit) {
+    S.batch_submit(P, a, b, c, prm.exact);
   } else {
     launch_mat_mult(S, P, a, b, c, prm.exact);
   }

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <functional>
 #include <map>
 #include <memory>
 #include <stdexcept>
@@ -217,7 +218,6 @@ struct MixedPlan {
   int n_groups[4] = {-1, -1, -1, -1};   // groups of 1, 2, 4 and 8 output blocks (-1: not built yet)
   int tuned_g = -1;                 // group size chosen by the autotuner (index into 1, 2, 4, 8)
   int kernel = -1;                  // 0 = tcgen05 tiles, 1 = per-block mma.sync (-1: not chosen yet)
-  float kernel_ms[2] = {0, 0};      // their timed milliseconds when the choice was made by timing
   float tune_ms[4] = {0, 0, 0, 0};
   int64_t n_pairs = 0, flops = 0;
   DevBuf<int64_t> own_ptr;        // type 2 only (type 1 uses the FP64 plan's lists, already sorted)
@@ -286,7 +286,7 @@ struct System {
   std::map<std::pair<int, int>, FragBuf> frags;   // (range, slot) fragment buffers of the mixed products
   std::map<std::tuple<int, int, int, int>, std::unique_ptr<UmmaPlan>> uplans;   // tensor-core tile plans
   int mixed_kernel = -1;          // split-precision products: 0 = tcgen05 tiles (umma.cu), 1 = mma.sync per block,
-                                  // -1 = the faster of the two, timed per product
+                                  // -1 = chosen per product by the tile plan's useful fraction
   int* umma_err_host = nullptr;   // mapped host word set by a tensor-core product whose bounded wait ran out
   int* umma_err_dev = nullptr;
   cudaStream_t stream = nullptr;  // the stream all work of the system is enqueued on
@@ -307,6 +307,9 @@ struct System {
                                   // other block sizes: 0 = generic warp per block, 4 = warp per block with
                                   // 4 x 2 register tiles per lane
   bool blocking_sync = false;     // host waits sleep on a blocking-sync event instead of spinning
+  // when set (batched serving), the chain's FP64 products go through this call instead of their own
+  // launch: it joins them to the products of other systems in one persistent launch
+  std::function<void(ProductPlan&, double*, const double*, double*, int)> batch_submit;
   cudaEvent_t sync_ev = nullptr;
   ProductProfile prof;
   ~System();
@@ -329,6 +332,16 @@ MixedPlan& get_mixed_plan(System& S, int mult_type, int ra, int rb, int rc);
 
 // mult.cu
 void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, double* c, int exact);
+struct BatchItem {                 // one FP64 product of a batched launch (roles of launch_mat_mult)
+  System* S;
+  ProductPlan* P;
+  double* a;
+  const double* b;
+  double* c;
+  int exact;
+};
+void launch_mat_mult_batch(const std::vector<BatchItem>& items, cudaStream_t st);
+void ensure_product_order(System& S, ProductPlan& P);   // the 4 x 4 kernels' output order (built once)
 
 // gen.cu: synthetic S (which = 0) or H (which = 1) of range r into out
 void generate_SH(System& S, int r, int which, uint64_t seed, double* out);

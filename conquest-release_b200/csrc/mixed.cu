@@ -250,44 +250,25 @@ static void mat_mult_mma_sync(System& S, MixedPlan& MP, int mult_type, int ra, i
   launch_mult_tc(S, MP, fx.hi.p, fx.lo.p, fb.hi.p, fb.lo.p, out);
 }
 
-// Kernel choice of a split-precision product: the system's setting, or (setting -1) the faster of the
-// tcgen05 tiles and the per-block mma.sync kernel, timed on the product's first call (each warm
-// once, then the better of two timed launches each; both write the whole output).
+// Kernel choice of a split-precision product: the system's setting, or (setting -1) a fixed rule on
+// the product's tile plan, so that a product always runs the same kernel (and gives the same bits)
+// whatever else runs on the device: the tcgen05 tiles where at least kTileMinFill of their issued
+// tensor work is useful (3 x the product's flops / issued flops), else the per-block mma.sync kernel.
+// Measured on B200: the tiles issue 300-800 TFLOP/s and the per-block kernel about 170 at a useful
+// fraction near 0.5, so the tiles pay above roughly 0.15.
+constexpr double kTileMinFill = 0.15;
+
 void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c) {
   MixedPlan& MP = get_mixed_plan(S, mult_type, ra, rb, rc);
-  const bool tiles_ok = S.max_nsf > 0 && umma_usable(S, mult_type, ra, rb, rc);
+  const bool tiles_ok = umma_usable(S, mult_type, ra, rb, rc);
   int k = S.mixed_kernel;
   if (k == 0 && !tiles_ok) k = 1;
   if (k < 0) {
     if (MP.kernel < 0) {
-      if (!tiles_ok) {
-        MP.kernel = 1;
-      } else {
-        cudaEvent_t e0, e1;
-        CQ_CUDA(cudaEventCreate(&e0));
-        CQ_CUDA(cudaEventCreate(&e1));
-        float best[2] = {1e30f, 1e30f};
-        for (int kk = 0; kk < 2; ++kk) {
-          auto run = [&] {
-            if (kk == 0) mat_mult_umma(S, mult_type, ra, rb, rc, a, b, c);
-            else mat_mult_mma_sync(S, MP, mult_type, ra, rb, rc, a, b, c);
-          };
-          run();
-          for (int rep = 0; rep < 2; ++rep) {
-            CQ_CUDA(cudaEventRecord(e0, S.stream));
-            run();
-            CQ_CUDA(cudaEventRecord(e1, S.stream));
-            CQ_CUDA(cudaEventSynchronize(e1));
-            float ms = 0.f;
-            CQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            best[kk] = std::min(best[kk], ms);
-          }
-        }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        MP.kernel_ms[0] = best[0];
-        MP.kernel_ms[1] = best[1];
-        MP.kernel = best[0] <= best[1] ? 0 : 1;
+      MP.kernel = 1;
+      if (tiles_ok) {
+        const UmmaPlan& U = get_umma_plan(S, mult_type, ra, rb, rc);
+        if (U.issued_flops > 0 && 3.0 * (double)U.flops / (double)U.issued_flops >= kTileMinFill) MP.kernel = 0;
       }
     }
     k = MP.kernel;

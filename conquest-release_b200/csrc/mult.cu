@@ -13,8 +13,12 @@
 // the launch shape.
 //
 // The bound is the L2/HBM traffic of the operand blocks (an nd x nd FP64 block
-// pair per triple, 2 nd^3 flops): for nd = 4 this is 256 B per 128 flops.
+// pair per triple, 2 nd^3 flops): for nd = 4 this is 256 B per 128 flops.  The 4 x 4 kernels write
+// their output blocks with streaming (evict-first) stores: an output range is often larger than L2
+// (the 42-bohr range of the 512-atom cell: 152 MB) and would otherwise push the operand blocks,
+// which every output block re-reads, out of L2.
 #include <algorithm>
+#include <memory>
 #include <numeric>
 
 #include "cq_internal.hpp"
@@ -178,7 +182,7 @@ __global__ void __launch_bounds__(128) k_mult_nd4_tpb(MultArgs M) {
   }
   double2* O2 = reinterpret_cast<double2*>(M.out + 16 * (int64_t)q);
 #pragma unroll
-  for (int v = 0; v < 8; ++v) O2[v] = make_double2(acc[2 * v], acc[2 * v + 1]);
+  for (int v = 0; v < 8; ++v) __stcs(O2 + v, make_double2(acc[2 * v], acc[2 * v + 1]));
 }
 
 // 4 x 4 blocks, one thread per output block, the first operand's row staged in shared memory.
@@ -248,7 +252,7 @@ __global__ void __launch_bounds__(128) k_mult_nd4_rows(MultArgs M, const int4* _
   if (q < d.y) {
     double2* O2 = reinterpret_cast<double2*>(M.out + 16 * (int64_t)q);
 #pragma unroll
-    for (int v = 0; v < 8; ++v) O2[v] = make_double2(acc[2 * v], acc[2 * v + 1]);
+    for (int v = 0; v < 8; ++v) __stcs(O2 + v, make_double2(acc[2 * v], acc[2 * v + 1]));
   }
 }
 
@@ -261,15 +265,16 @@ __global__ void __launch_bounds__(128) k_mult_nd4_rows(MultArgs M, const int4* _
 // per block: conflict-free 16-byte reads per quarter warp), then every lane does its own 4 x 4
 // product in the reference order.  Output blocks are taken in `order` (descending pair count)
 // so the lanes of a warp have pair lists of similar length.
+constexpr int kStageStride = 9;   // double2 per staged 4 x 4 block (8 + 1 padding)
+
+// One warp of the warp-staged 4 x 4 kernel: output slots [base, base + 32) of `order`, operand blocks
+// staged through X and B (32 x kStageStride double2 each, this warp's own shared memory).
 template <int TYPE, bool EXACT>
-__global__ void __launch_bounds__(128, 5) k_mult_nd4_warp(MultArgs M, const int* __restrict__ order) {
-  constexpr int kStride = 9;   // double2 per staged block (8 + 1 padding)
-  __shared__ double2 sx[4][32 * kStride];
-  __shared__ double2 sb[4][32 * kStride];
+__device__ __forceinline__ void warp_nd4_staged(const MultArgs& M, const int* __restrict__ order, int base, double2* X,
+                                                double2* B) {
+  constexpr int kStride = kStageStride;
   const unsigned kFull = 0xffffffffu;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int base = (blockIdx.x * 4 + warp) * 32;
-  if (base >= M.n_out) return;                  // whole warp
+  const int lane = threadIdx.x & 31;
   const int slot = base + lane;
   const bool has = slot < M.n_out;
   const int q = has ? order[slot] : 0;
@@ -277,8 +282,6 @@ __global__ void __launch_bounds__(128, 5) k_mult_nd4_warp(MultArgs M, const int*
   double acc[16];
 #pragma unroll
   for (int e = 0; e < 16; ++e) acc[e] = 0.0;
-  double2* X = sx[warp];
-  double2* B = sb[warp];
   const double2* Xg = reinterpret_cast<const double2*>(M.x);
   const double2* Bg = reinterpret_cast<const double2*>(M.b);
   const int chunk = lane & 7;
@@ -334,8 +337,18 @@ __global__ void __launch_bounds__(128, 5) k_mult_nd4_warp(MultArgs M, const int*
   if (has) {
     double2* O2 = reinterpret_cast<double2*>(M.out + 16 * (int64_t)q);
 #pragma unroll
-    for (int v = 0; v < 8; ++v) O2[v] = make_double2(acc[2 * v], acc[2 * v + 1]);
+    for (int v = 0; v < 8; ++v) __stcs(O2 + v, make_double2(acc[2 * v], acc[2 * v + 1]));
   }
+}
+
+template <int TYPE, bool EXACT>
+__global__ void __launch_bounds__(128, 5) k_mult_nd4_warp(MultArgs M, const int* __restrict__ order) {
+  __shared__ double2 sx[4][32 * kStageStride];
+  __shared__ double2 sb[4][32 * kStageStride];
+  const int warp = threadIdx.x >> 5;
+  const int base = (blockIdx.x * 4 + warp) * 32;
+  if (base >= M.n_out) return;                  // whole warp
+  warp_nd4_staged<TYPE, EXACT>(M, order, base, sx[warp], sb[warp]);
 }
 
 // Uniform 4 x 4 blocks, four lanes per output block: lane m of a quad owns column m of the block
@@ -405,8 +418,8 @@ __global__ void __launch_bounds__(128, 8) k_mult_nd4_quad(MultArgs M, const int*
   }
   if (has) {
     double2* O2 = reinterpret_cast<double2*>(M.out + 16 * (int64_t)q) + 2 * m;
-    O2[0] = make_double2(acc[0], acc[1]);
-    O2[1] = make_double2(acc[2], acc[3]);
+    __stcs(O2, make_double2(acc[0], acc[1]));
+    __stcs(O2 + 1, make_double2(acc[2], acc[3]));
   }
 }
 
@@ -415,9 +428,8 @@ __global__ void __launch_bounds__(128, 8) k_mult_nd4_quad(MultArgs M, const int*
 // so per term of the inner sum a lane loads 4 + 2 operand values for 8 multiply-adds instead of
 // 2 per multiply-add.  The order of the terms of every element is unchanged.
 template <int TYPE, bool EXACT>
-__global__ void __launch_bounds__(256) k_mult_tile(MultArgs M) {
-  const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (q >= M.n_out) return;
+__device__ __forceinline__ void warp_tile(const MultArgs& M, int q) {
+  const int lane = threadIdx.x & 31;
   const int ndi = M.prim_nsf[M.o_row[q]];
   const int ndo = M.cover_nsf[M.o_cover[q]];     // type 1: nd_j ; type 2: nd_k
   const int nct = (ndo + 1) >> 1, nrt = (ndi + 3) >> 2;
@@ -476,6 +488,59 @@ __global__ void __launch_bounds__(256) k_mult_tile(MultArgs M) {
   }
 }
 
+template <int TYPE, bool EXACT>
+__global__ void __launch_bounds__(256) k_mult_tile(MultArgs M) {
+  const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (q >= M.n_out) return;
+  warp_tile<TYPE, EXACT>(M, q);
+}
+
+// Many independent products in one persistent launch (the concatenation of their output-block
+// lists): every warp takes work units u = warp id, warp id + warps in the grid, ...; a unit is 32
+// output slots of a uniform 4 x 4 product (the warp-staged kernel) or one output block of any other
+// product (the register-tiled kernel).  Each output block is computed by exactly the operations of the
+// single-product kernels, so the results are the same bits as separate launches.  The product table
+// travels in the kernel's parameters (no host-to-device copy before the launch).
+struct BatchProduct {
+  MultArgs M;
+  const int* order;                // 4 x 4 products: output blocks by descending pair count
+  int kind;                        // bit 0: type 2, bit 1: exact rounding, bit 2: uniform 4 x 4 blocks
+};
+constexpr int kBatchMax = 96;      // products per launch (the table stays within the 32 KB parameter space)
+struct BatchParams {
+  int n_prod;
+  int unit_off[kBatchMax + 1];     // first work unit of each product; unit_off[n_prod] = all units
+  BatchProduct prods[kBatchMax];
+};
+static_assert(sizeof(BatchParams) < 32000, "batched product table exceeds the kernel parameter space");
+
+__global__ void __launch_bounds__(128, 5) k_mult_batch(const __grid_constant__ BatchParams B) {
+  __shared__ double2 sx[4][32 * kStageStride];
+  __shared__ double2 sb[4][32 * kStageStride];
+  const int warp = threadIdx.x >> 5;
+  const int n_units = B.unit_off[B.n_prod];
+  for (int u = blockIdx.x * 4 + warp; u < n_units; u += gridDim.x * 4) {
+    int lo = 0, hi = B.n_prod - 1;               // product of unit u: last p with unit_off[p] <= u
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (B.unit_off[mid] <= u) lo = mid; else hi = mid - 1;
+    }
+    const BatchProduct& P = B.prods[lo];
+    const int kind = P.kind;
+    const int first = (u - B.unit_off[lo]) * ((kind & 4) ? 32 : 1);
+    switch (kind) {
+      case 0: warp_tile<1, false>(P.M, first); break;
+      case 1: warp_tile<2, false>(P.M, first); break;
+      case 2: warp_tile<1, true>(P.M, first); break;
+      case 3: warp_tile<2, true>(P.M, first); break;
+      case 4: warp_nd4_staged<1, false>(P.M, P.order, first, sx[warp], sb[warp]); break;
+      case 5: warp_nd4_staged<2, false>(P.M, P.order, first, sx[warp], sb[warp]); break;
+      case 6: warp_nd4_staged<1, true>(P.M, P.order, first, sx[warp], sb[warp]); break;
+      default: warp_nd4_staged<2, true>(P.M, P.order, first, sx[warp], sb[warp]); break;
+    }
+  }
+}
+
 // One drop-in m_kern_max (type 1) / m_kern_min (type 2) call: output blocks with explicit
 // offsets, accumulated in place in the layouts mat_mult passes (type 1 reads the local
 // transpose a(n3 + nd3*n1); type 2 accumulates into it).  One warp per output block.
@@ -520,6 +585,17 @@ void launch_dropin(int type, const int64_t* d_out, const int* d_dims, const int6
   CQ_CUDA(cudaGetLastError());
 }
 
+// output blocks by descending pair count (stable): lanes of a warp get similar list lengths
+static void ensure_order(System& S, ProductPlan& P) {
+  if (P.order.n != 0) return;
+  std::vector<int64_t> ptr = P.ptr.download(S.stream);
+  const int n_out = (int)ptr.size() - 1;
+  std::vector<int> ord(std::max(n_out, 0));
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int u, int v) { return ptr[u + 1] - ptr[u] > ptr[v + 1] - ptr[v]; });
+  P.order.upload(ord, S.stream);
+}
+
 // One launch of the FP64 product with kernel `variant` (0..3 and 5 for uniform 4 x 4 blocks with
 // 16-byte aligned operands; anything else runs the generic kernel).  All variants give the same
 // bits: they differ only in how the work is mapped onto the GPU.
@@ -528,14 +604,7 @@ static void launch_variant(System& S, ProductPlan& P, const MultArgs& M, int var
   const int T = 256;
   RangeIndex& O = P.mult_type == 1 ? *S.ranges[P.rc] : *S.ranges[P.ra];
   RangeIndex& X = P.mult_type == 1 ? *S.ranges[P.ra] : *S.ranges[P.rc];
-  if (nd4 && (variant == 3 || variant == 5) && P.order.n == 0) {
-    // output blocks by descending pair count (stable): lanes of a warp get similar list lengths
-    std::vector<int64_t> ptr = P.ptr.download(st);
-    std::vector<int> ord(M.n_out);
-    std::iota(ord.begin(), ord.end(), 0);
-    std::stable_sort(ord.begin(), ord.end(), [&](int u, int v) { return ptr[u + 1] - ptr[u] > ptr[v + 1] - ptr[v]; });
-    P.order.upload(ord, st);
-  }
+  if (nd4 && (variant == 3 || variant == 5)) ensure_order(S, P);
   if (nd4 && variant == 5) {
     const int grid = (M.n_out + 31) / 32;        // 8 output blocks per warp, 4 warps per CTA
     if (P.mult_type == 1) {
@@ -646,7 +715,9 @@ static int tuned_variant(System& S, ProductPlan& P, const MultArgs& M, int exact
   return P.tuned;
 }
 
-void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, double* c, int exact) {
+// kernel arguments of one product (roles of mat_mult: type 1 writes c from a, b; type 2 writes a from c, b);
+// nd4: uniform 4 x 4 blocks with 16-byte aligned operands (the 4 x 4 kernels read 16-byte vectors)
+static MultArgs product_args(System& S, ProductPlan& P, double* a, const double* b, double* c, bool* nd4) {
   RangeIndex &A = *S.ranges[P.ra], &B = *S.ranges[P.rb], &C = *S.ranges[P.rc];
   MultArgs M;
   M.ptr = P.ptr.p;
@@ -663,11 +734,17 @@ void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, doub
   M.x_cover = X.nb_cover.p; M.x_elem = X.nb_elem.p;
   M.x = P.mult_type == 1 ? a : c;
   M.out = P.mult_type == 1 ? c : a;
+  const bool aligned = ((uintptr_t)b % 16 == 0) && ((uintptr_t)M.x % 16 == 0) && ((uintptr_t)M.out % 16 == 0);
+  *nd4 = S.uniform_nsf == 4 && aligned;
+  return M;
+}
+
+void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, double* c, int exact) {
+  RangeIndex &A = *S.ranges[P.ra], &B = *S.ranges[P.rb], &C = *S.ranges[P.rc];
+  bool nd4 = false;
+  MultArgs M = product_args(S, P, a, b, c, &nd4);
   if (M.n_out == 0) return;
   cudaStream_t st = S.stream;
-  // the 4 x 4 kernels read blocks with 16-byte vector loads: require 16-byte aligned operands
-  const bool aligned = ((uintptr_t)b % 16 == 0) && ((uintptr_t)M.x % 16 == 0) && ((uintptr_t)M.out % 16 == 0);
-  const bool nd4 = S.uniform_nsf == 4 && aligned;
   int variant = S.mult_variant;
   if (variant == kVariantAuto) variant = tuned_variant(S, P, M, exact, nd4);
   cudaEvent_t ev0 = nullptr;
@@ -680,6 +757,49 @@ void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, doub
     double bytes = 8.0 * (double)(A.length + B.length + C.length);
     S.prof.recs.push_back({ev0, ev1, bytes, (double)P.flops});
   }
+}
+
+void ensure_product_order(System& S, ProductPlan& P) {
+  if (S.uniform_nsf == 4) ensure_order(S, P);
+}
+
+// Products of independent systems (or of one system) in persistent launches on `st` (up to kBatchMax
+// products each).  The caller orders `st` after the work the operands depend on and the systems' later
+// work after it.
+void launch_mat_mult_batch(const std::vector<BatchItem>& items, cudaStream_t st) {
+  int dev_id = 0, sms = 0, occ = 0;
+  CQ_CUDA(cudaGetDevice(&dev_id));
+  CQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id));
+  CQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mult_batch, 128, 0));
+  auto params = std::make_unique<BatchParams>();
+  BatchParams& B = *params;
+  auto flush = [&] {
+    if (B.n_prod == 0) return;
+    const int n_units = B.unit_off[B.n_prod];
+    const int grid = std::max(1, std::min(sms * std::max(occ, 1), (n_units + 3) / 4));
+    k_mult_batch<<<grid, 128, 0, st>>>(B);
+    CQ_CUDA(cudaGetLastError());
+    B.n_prod = 0;
+  };
+  B.n_prod = 0;
+  B.unit_off[0] = 0;
+  for (const BatchItem& it : items) {
+    System& S = *it.S;
+    ProductPlan& P = *it.P;
+    bool nd4 = false;
+    BatchProduct bp;
+    bp.M = product_args(S, P, it.a, it.b, it.c, &nd4);
+    if (bp.M.n_out == 0) continue;
+    if (nd4) ensure_order(S, P);
+    bp.order = nd4 ? P.order.p : nullptr;
+    bp.kind = (P.mult_type == 2 ? 1 : 0) | (it.exact ? 2 : 0) | (nd4 ? 4 : 0);
+    if (B.n_prod == kBatchMax) { flush(); B.unit_off[0] = 0; }
+    B.prods[B.n_prod] = bp;
+    B.unit_off[B.n_prod + 1] = B.unit_off[B.n_prod] + (nd4 ? (bp.M.n_out + 31) / 32 : bp.M.n_out);
+    ++B.n_prod;
+    S.launches++;
+  }
+  flush();
 }
 
 cudaEvent_t ProductProfile::get() {

@@ -26,6 +26,92 @@ int guarded_call(const std::function<void()>& f);
 
 namespace {
 
+// Gathers the FP64 products of the slots' solves and runs each gathering as one persistent launch
+// over the concatenated output-block lists (launch_mat_mult_batch) on the batcher's own stream.  A
+// product's system stream records an event the launch waits for, and waits for the launch's completion
+// event itself, so stream order is kept without host synchronisation.  A gathering is launched as soon
+// as every solving slot has a product waiting, or when the oldest waiting product has waited the
+// window; each product is computed exactly as alone, so the results do not change.
+class ProductBatcher {
+ public:
+  ProductBatcher(int device, double window_us) : window_(window_us > 0 ? window_us : 50.0) {
+    CQ_CUDA(cudaSetDevice(device));
+    CQ_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+  }
+  ~ProductBatcher() {
+    if (st_) { cudaStreamSynchronize(st_); cudaStreamDestroy(st_); }
+  }
+  void enter() { std::lock_guard<std::mutex> lk(mu_); ++active_; }
+  void leave() {
+    std::lock_guard<std::mutex> lk(mu_);
+    --active_;
+    if (!pending_.empty() && (int)pending_.size() >= active_) flush_locked();
+  }
+
+  void submit(System& S, ProductPlan& P, double* a, const double* b, double* c, int exact) {
+    ensure_product_order(S, P);
+    cudaEvent_t ready;
+    CQ_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    CQ_CUDA(cudaEventRecord(ready, S.stream));
+    auto ticket = std::make_shared<Ticket>();
+    std::unique_lock<std::mutex> lk(mu_);
+    pending_.push_back({BatchItem{&S, &P, a, b, c, exact}, ready, ticket});
+    const uint64_t gen = gen_;
+    if ((int)pending_.size() >= active_) {
+      flush_locked();
+    } else {
+      cv_.wait_for(lk, std::chrono::duration<double, std::micro>(window_), [&] { return gen_ != gen; });
+      if (gen_ == gen) flush_locked();
+    }
+    lk.unlock();
+    if (!ticket->error.empty()) throw Error(ticket->code, ticket->error);
+    CQ_CUDA(cudaStreamWaitEvent(S.stream, ticket->done->e, 0));
+  }
+
+ private:
+  struct Event {
+    cudaEvent_t e = nullptr;
+    ~Event() { if (e) cudaEventDestroy(e); }
+  };
+  struct Ticket {
+    std::shared_ptr<Event> done;
+    std::string error;
+    int code = 0;
+  };
+  struct Pending {
+    BatchItem item;
+    cudaEvent_t ready;
+    std::shared_ptr<Ticket> ticket;
+  };
+  void flush_locked() {
+    std::vector<BatchItem> items;
+    auto done = std::make_shared<Event>();
+    try {
+      for (auto& p : pending_) {
+        CQ_CUDA(cudaStreamWaitEvent(st_, p.ready, 0));
+        items.push_back(p.item);
+      }
+      launch_mat_mult_batch(items, st_);
+      CQ_CUDA(cudaEventCreateWithFlags(&done->e, cudaEventDisableTiming));
+      CQ_CUDA(cudaEventRecord(done->e, st_));
+      for (auto& p : pending_) p.ticket->done = done;
+    } catch (const Error& e) {
+      for (auto& p : pending_) { p.ticket->error = e.what(); p.ticket->code = e.code; }
+    }
+    for (auto& p : pending_) cudaEventDestroy(p.ready);
+    pending_.clear();
+    ++gen_;
+    cv_.notify_all();
+  }
+  double window_;
+  cudaStream_t st_ = nullptr;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::vector<Pending> pending_;
+  int active_ = 0;
+  uint64_t gen_ = 0;
+};
+
 struct Request {
   int64_t id = 0;
   int n = 0;
@@ -110,6 +196,7 @@ class Server {
     if (!c.dry_run) {
       CQ_CUDA(cudaGetDevice(&device_));
       init_device_pool();
+      if (c.batch_products) batcher_ = std::make_unique<ProductBatcher>(device_, c.batch_window_us);
     }
     for (int s = 0; s < c.n_slots; ++s) workers_.emplace_back([this, s] { worker(s); });
   }
@@ -247,9 +334,20 @@ class Server {
       for (int r = 0; r < LNVSolver::NR; ++r) idx[r] = r;
       cq_lnv_params prm = cfg_.lnv;
       prm.mixed = q.mixed;
+      if (batcher_) {
+        prm.graphs = 0;             // products leave the system's stream: no graph capture
+        S.batch_submit = [this, &S](ProductPlan& P, double* a, const double* b, double* c, int exact) {
+          batcher_->submit(S, P, a, b, c, exact);
+        };
+      }
       LNVSolver L(S, idx, q.ne_spin, prm);
       generate_SH(S, LNVSolver::RS, 0, q.seed, L.Smat.p);
       generate_SH(S, LNVSolver::RH, 1, q.seed, L.Hmat.p);
+      struct Active {              // this slot counts as solving while its chain runs
+        ProductBatcher* b;
+        explicit Active(ProductBatcher* x) : b(x) { if (b) b->enter(); }
+        ~Active() { if (b) b->leave(); }
+      } active(batcher_.get());
       L.solve();
       host_wait(S);
       const LNVStats& s = L.stats;
@@ -280,6 +378,7 @@ class Server {
   int running_ = 0;
   bool stop_ = false;
   std::vector<std::thread> workers_;
+  std::unique_ptr<ProductBatcher> batcher_;   // declared last: destroyed after the workers are joined
 };
 
 }  // namespace cqb
@@ -302,6 +401,8 @@ int cq_server_config_default(cq_server_config* c) {
   c->dry_run = 0;
   c->dry_run_seconds = 0.01;
   cq_lnv_params_default(&c->lnv);
+  c->batch_products = 0;
+  c->batch_window_us = 50.0;
   return CQ_OK;
 }
 

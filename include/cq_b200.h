@@ -110,6 +110,20 @@ int cq_export_radius(cq_system* sys, int r, double* out, int64_t cap, int64_t* n
 int cq_mat_mult(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a_dev, const double* b_dev,
                 double* c_dev, int precision);
 
+/*
+ * Batched products (no counterpart in the reference, which runs one mat_mult at a time): n
+ * independent FP64 products (precision[k] CQ_PREC_FP64 or CQ_PREC_FP64_FMA), each on its own system
+ * or on one system with different operands, run as ONE persistent kernel over the concatenation of
+ * their output-block lists.  Product k has the arguments of cq_mat_mult on systems[k].  Every output
+ * element sees the same operations as in cq_mat_mult, so the results are bit-identical to n separate
+ * calls.  The launch is enqueued on systems[0]'s stream after the work already enqueued on every
+ * system's stream, and later work on every system's stream waits for it.  The call waits for the
+ * copy of the launch's small descriptor table (not for the products).
+ */
+int cq_mat_mult_batch(int n, cq_system* const* systems, const int* mult_type, const int* ra, const int* rb,
+                      const int* rc, double* const* a_dev, const double* const* b_dev, double* const* c_dev,
+                      const int* precision);
+
 /* Same as cq_mat_mult with host arrays: copies in, multiplies, copies the result out, synchronises. */
 int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c,
                      int precision);
@@ -246,10 +260,11 @@ int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out)
  * spins in cudaStreamSynchronize (default, lowest latency for one solver). */
 #define CQ_OPT_MULT_VARIANT 1
 #define CQ_OPT_BLOCKING_SYNC 2
-/* CQ_OPT_MIXED_KERNEL: kernel of the CQ_PREC_BF16X3 products.  -1 (default) = the faster of the two
- * below, timed on each product's first call; 0 = dense 128 x 128 tiles on the tcgen05 tensor cores
- * with TMEM accumulators (every block size 4..128; other systems use 1); 1 = one padded 16 x 16
- * block per warp-level mma.sync (block sizes up to 16). */
+/* CQ_OPT_MIXED_KERNEL: kernel of the CQ_PREC_BF16X3 products.  -1 (default) = chosen per product
+ * by a fixed rule (the tiles where at least 15 % of their issued tensor work is useful), so a product
+ * always gives the same bits; 0 = dense 128 x 128 tiles on the tcgen05 tensor cores with TMEM
+ * accumulators, operands staged by bulk copies (every block size 4..16; other systems use 1);
+ * 1 = one padded 16 x 16 block per warp-level mma.sync. */
 #define CQ_OPT_MIXED_KERNEL 3
 int cq_system_set_option(cq_system* sys, int option, int value);
 
@@ -423,6 +438,10 @@ typedef struct {
                               dry_run_seconds (scheduler tests without a GPU) */
   double dry_run_seconds;
   cq_lnv_params lnv;       /* solver parameters of every request (lnv.mixed is overridden) */
+  int batch_products;      /* 1: the FP64 products of the slots' solves are gathered and run together,
+                              one persistent launch per gathering (cq_mat_mult_batch; CUDA graphs of
+                              the LNV calls off); a product waits at most batch_window_us for others */
+  double batch_window_us;
 } cq_server_config;
 
 typedef struct {

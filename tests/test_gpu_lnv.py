@@ -234,3 +234,31 @@ def test_system_outlives_its_solvers():
     assert not g.handle.value
     glnv.close()                                    # nothing left to destroy
     assert not glnv._h.value
+
+
+GOLDEN512_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "lnv_chain_si512.json")
+
+
+def test_benchmark_workload_matches_oracle_chain():
+    """The benchmark workload itself (512-atom Si supercell, 4x4 blocks, S/H/L/T ranges 10/12/16/10 bohr,
+    1024 electrons, 50 LNV iterations, tolerance 1e-7): the GPU solve against the oracle chain's fixture.
+    Products are bit-exact and every reduction exact on both sides, so the chains take the same steps:
+    the same number of products, the same final L to the bit, E and Ne within 1e-10."""
+    import cq_b200
+    gold = json.load(open(GOLDEN512_PATH))["cases"]["r10_12_16_10"]
+    coords, cell = inputs.diamond_si(4, sigma=0.1, seed=2)
+    n = len(coords)
+    rng = cq_b200.lnv_ranges(*gold["ranges"])
+    ridx = {k: i for i, k in enumerate(rng)}
+    g = cq_b200.System(coords, cell, np.full(n, 4, np.int32), list(rng.values()))
+    S = inputs.overlap_S(g.blocklist(ridx["S"], coords, cell))
+    H = inputs.hamiltonian_H(g.blocklist(ridx["H"], coords, cell), seed=5)
+    solver = cq_b200.LNV(g, ridx, gold["ne_spin"], exact=1, max_outer=gold["max_outer"])
+    res, L, _ = solver.solve_host(S, H, want_L=True)
+    assert res["converged"] == int(gold["converged"])
+    assert res["n_products"] == gold["n_products"]
+    assert L.size == gold["L_length"]
+    assert hashlib.sha256(np.ascontiguousarray(L, np.float64).tobytes()).hexdigest() == gold["L_sha256"]
+    assert abs(res["energy"] - gold["energy"]) <= 1e-10 * abs(gold["energy"])
+    assert abs(res["electrons"] - gold["electrons"]) <= 1e-10 * abs(gold["electrons"])
+    solver.close()

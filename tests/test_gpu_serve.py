@@ -40,6 +40,22 @@ def _key(r):
     return (r["energy"], r["electrons"], r["n_products"], r["flops"], r["n_products_mixed"], r["converged"])
 
 
+def test_batched_products_alone_equals_mix():
+    """Four slots whose FP64 products are gathered into shared persistent launches (batch_products)
+    give the same bits as a one-slot server without gathering: the gathered launches compute every
+    output block exactly as a product of its own."""
+    reqs = _requests()
+    alone = cq_b200.Server(n_slots=1, max_outer=3)
+    ra = _run(alone, reqs)
+    alone.close()
+    mix = cq_b200.Server(n_slots=4, max_outer=3, batch_products=True, batch_window_us=100.0)
+    rm = _run(mix, reqs)
+    mix.close()
+    for a, m in zip(ra, rm):
+        assert a["status"] == 0 and m["status"] == 0, (a["message"], m["message"])
+        assert _key(a) == _key(m)
+
+
 def test_alone_equals_mix():
     reqs = _requests()
     alone = cq_b200.Server(n_slots=1, max_outer=3)
