@@ -91,6 +91,8 @@ def lib():
         "cq_export_index": [c_void_p, c_int, ctypes.c_char_p, P(c_int64), c_int64, P(c_int64)],
         "cq_export_radius": [c_void_p, c_int, P(c_double), c_int64, P(c_int64)],
         "cq_mat_mult": [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int],
+        "cq_m_kern_defer": [c_int],
+        "cq_m_kern_flush": [],
         "cq_mat_mult_batch": [c_int, P(c_void_p), P(c_int), P(c_int), P(c_int), P(c_int), P(c_void_p), P(c_void_p),
                               P(c_void_p), P(c_int)],
         "cq_mat_mult_host": [c_void_p, c_int, c_int, c_int, c_int, P(c_double), P(c_double), P(c_double), c_int],
@@ -397,6 +399,16 @@ def m_kern(kind, k_off, kpart, ib_nd_acc, ibaddr, nbnab, ibpart, ibseq, bndim2, 
     check(f(int(k_off), int(kpart), *[_ip(x) for x in arrs], _dp(a), _dp(b), _dp(c), *[_ip(x) for x in ah],
             *[_ip(x) for x in ch], int(chalo["ni_in_halo"]), *[_ip(x) for x in tr], int(mx_absb), int(mx_part),
             int(mx_iprim), a.size, b.size, c.size))
+
+
+def m_kern_defer(np_in_halo):
+    """cq_m_kern_defer: >0 = the following m_kern calls of one partition loop enqueue their work and the call
+    with kpart == np_in_halo completes the loop; 0 = complete every call (flushes an open loop)."""
+    check(lib().cq_m_kern_defer(int(np_in_halo)))
+
+
+def m_kern_flush():
+    check(lib().cq_m_kern_flush())
 
 
 def mat_mult_batch(products):

@@ -421,6 +421,114 @@ int cq_launch_count(cq_system* sys, int64_t* count) {
   return guarded([&] { check_sys(sys); CQ_CHECK(count, CQ_ERR_ARG, "null argument"); *count = sys->S.launches; });
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Deferred drop-in calls (cq_m_kern_defer): the device copies of a and c live across the partition
+// loop of one mat_mult, each call copies only its partition's b and block lists (through pinned,
+// double-buffered staging) and enqueues its arithmetic on the drop-in stream, and the call of the
+// last partition copies the result back and synchronises.  Buffers grow and are reused: after the
+// first loop no call allocates.  Per calling thread.
+// ---------------------------------------------------------------------------
+struct PinnedBuf {
+  unsigned char* p = nullptr;
+  size_t n = 0;
+  cudaEvent_t used = nullptr;      // recorded after the copy that last read this buffer
+  void reserve(size_t bytes) {
+    if (bytes <= n) return;
+    if (p) cudaFreeHost(p);
+    p = nullptr; n = 0;
+    CQ_CUDA(cudaMallocHost((void**)&p, bytes));
+    n = bytes;
+  }
+  ~PinnedBuf() {
+    if (used) cudaEventDestroy(used);
+    if (p) cudaFreeHost(p);
+  }
+};
+
+struct DropinState {
+  int np = 0;                      // A-halo partitions of the current loop (0: complete every call)
+  int type = 0;
+  bool open = false;               // a loop's device copies hold pending work
+  double* host_out = nullptr;      // result array of the open loop (c for max, a for min)
+  int64_t len_out = 0;
+  cudaStream_t st = nullptr;
+  DevBuf<double> da, db, dc;
+  DevBuf<unsigned char> didx;
+  PinnedBuf stage[2];
+  int turn = 0;
+  ~DropinState() {
+    if (st) { cudaStreamSynchronize(st); }
+  }
+};
+static thread_local DropinState t_dropin;
+
+template <class T>
+static void grow(DevBuf<T>& b, size_t n, cudaStream_t st) {
+  if (b.n < n) b.alloc(n, st);
+}
+
+static void dropin_flush(DropinState& D) {
+  if (!D.open) return;
+  D.open = false;
+  const double* src = D.type == 1 ? D.dc.p : D.da.p;
+  if (D.len_out) CQ_CUDA(cudaMemcpyAsync(D.host_out, src, sizeof(double) * D.len_out, cudaMemcpyDeviceToHost, D.st));
+  CQ_CUDA(cudaStreamSynchronize(D.st));
+}
+
+static void dropin_deferred(DropinState& D, int type, int kpart, const std::vector<int64_t>& out_off,
+                            const std::vector<int>& dims, const std::vector<int64_t>& ptr,
+                            const std::vector<int64_t>& pairs, double* a, const double* b, double* c, int lena,
+                            int lenb, int lenc) {
+  if (!D.st) CQ_CUDA(cudaStreamCreateWithFlags(&D.st, cudaStreamNonBlocking));
+  if (kpart == 1 || !D.open) {
+    dropin_flush(D);                 // a loop left without its last partition completes here
+    D.type = type;
+    D.host_out = type == 1 ? c : a;
+    D.len_out = type == 1 ? lenc : lena;
+    grow(D.da, (size_t)std::max(lena, 1), D.st);
+    grow(D.dc, (size_t)std::max(lenc, 1), D.st);
+    CQ_CUDA(cudaMemcpyAsync(D.da.p, a, sizeof(double) * lena, cudaMemcpyHostToDevice, D.st));
+    CQ_CUDA(cudaMemcpyAsync(D.dc.p, c, sizeof(double) * lenc, cudaMemcpyHostToDevice, D.st));
+    CQ_CUDA(cudaStreamSynchronize(D.st));   // the caller may reuse a and c only after their copies
+    D.open = true;
+  }
+  CQ_CHECK(type == D.type, CQ_ERR_STATE, "m_kern: mult type changed inside a deferred partition loop");
+  const int n_out = (int)out_off.size();
+  if (n_out > 0) {
+    // staging: b of this partition, then the block lists (8-byte aligned sections)
+    const size_t sb = sizeof(double) * lenb, so = sizeof(int64_t) * out_off.size(), sp = sizeof(int64_t) * ptr.size(),
+                 sq = sizeof(int64_t) * pairs.size(), sd = ((sizeof(int) * dims.size() + 7) / 8) * 8;
+    const size_t total = sb + so + sp + sq + sd;
+    PinnedBuf& P = D.stage[D.turn];
+    D.turn ^= 1;
+    if (P.used) CQ_CUDA(cudaEventSynchronize(P.used));   // the copy that last read this buffer is done
+    P.reserve(total);
+    unsigned char* h = P.p;
+    std::memcpy(h, b, sb);
+    std::memcpy(h + sb, out_off.data(), so);
+    std::memcpy(h + sb + so, ptr.data(), sp);
+    std::memcpy(h + sb + so + sp, pairs.data(), sq);
+    std::memcpy(h + sb + so + sp + sq, dims.data(), sizeof(int) * dims.size());
+    grow(D.didx, total - sb + 8, D.st);
+    grow(D.db, (size_t)std::max(lenb, 1), D.st);
+    CQ_CUDA(cudaMemcpyAsync(D.db.p, h, sb, cudaMemcpyHostToDevice, D.st));
+    CQ_CUDA(cudaMemcpyAsync(D.didx.p, h + sb, total - sb, cudaMemcpyHostToDevice, D.st));
+    if (!P.used) CQ_CUDA(cudaEventCreateWithFlags(&P.used, cudaEventDisableTiming));
+    CQ_CUDA(cudaEventRecord(P.used, D.st));
+    const int64_t* d_out = reinterpret_cast<const int64_t*>(D.didx.p);
+    const int64_t* d_ptr = d_out + out_off.size();
+    const int64_t* d_pairs = d_ptr + ptr.size();
+    const int* d_dims = reinterpret_cast<const int*>(d_pairs + pairs.size());
+    if (type == 1) launch_dropin(1, d_out, d_dims, d_ptr, d_pairs, n_out, D.da.p, D.db.p, D.dc.p, D.st);
+    else launch_dropin(2, d_out, d_dims, d_ptr, d_pairs, n_out, D.dc.p, D.db.p, D.da.p, D.st);
+  }
+  if (kpart == D.np) dropin_flush(D);
+}
+
+extern "C" {
+
 // ---------------------------------------------------------------------------
 // drop-in m_kern_max / m_kern_min: the loop nest of the default kernel walked
 // on the host to list the block triples of this partition (in order), the
@@ -478,7 +586,11 @@ static int dropin(int type, int k_off, int kpart, const int* ib_nd_acc, const in
         nabeg += nd1 * nd3;
       }
     }
-    if (tri.empty()) return;
+    if (tri.empty()) {
+      DropinState& D = t_dropin;
+      if (D.np > 0) dropin_deferred(D, type, kpart, {}, {}, {0}, {}, a, b, c, lena, lenb, lenc);
+      return;
+    }
     // group by output block, preserving order
     std::vector<int> order(tri.size());
     std::iota(order.begin(), order.end(), 0);
@@ -495,6 +607,11 @@ static int dropin(int type, int k_off, int kpart, const int* ib_nd_acc, const in
       pairs.push_back(T.x); pairs.push_back(T.b); pairs.push_back(T.kd);
     }
     ptr.push_back((int64_t)order.size());
+    DropinState& D = t_dropin;
+    if (D.np > 0) {
+      dropin_deferred(D, type, kpart, out_off, dims, ptr, pairs, a, b, c, lena, lenb, lenc);
+      return;
+    }
     cudaStream_t st = 0;
     DevBuf<int64_t> d_out, d_ptr, d_pairs;
     DevBuf<int> d_dims;
@@ -507,6 +624,19 @@ static int dropin(int type, int k_off, int kpart, const int* ib_nd_acc, const in
     else CQ_CUDA(cudaMemcpyAsync(a, da.p, sizeof(double) * lena, cudaMemcpyDeviceToHost, st));
     CQ_CUDA(cudaStreamSynchronize(st));
   });
+}
+
+int cq_m_kern_defer(int np_in_halo) {
+  return guarded([&] {
+    CQ_CHECK(np_in_halo >= 0, CQ_ERR_ARG, "np_in_halo must be >= 0");
+    DropinState& D = t_dropin;
+    if (np_in_halo == 0) dropin_flush(D);
+    D.np = np_in_halo;
+  });
+}
+
+int cq_m_kern_flush(void) {
+  return guarded([&] { dropin_flush(t_dropin); });
 }
 
 int cq_m_kern_max(int k_off, int kpart, const int* ib_nd_acc, const int* ibaddr, const int* nbnab, const int* ibpart,

@@ -251,6 +251,14 @@ struct UmmaPlan {
   DevBuf<unsigned int> rtabs, ktabs;   // row tables (row groups, column chunks); K tables of the units
   DevBuf<int> outmap, xtab, btab, xs_rtab, xs_unit, bs_rtab, bs_unit;
   DevBuf<uint4> xslabs, bslabs;   // packed bf16 operands, 8 KB per slab, rewritten by every product call
+  // host side of the plan, kept to build the slab tables and buffers on the product's first
+  // tensor-core call (a product that runs on the per-block kernel never allocates them)
+  bool materialised = false;
+  int mult_type = 1, ra = -1, rb = -1, rc = -1, n_groups = 0, n_chunks = 0;
+  std::vector<int2> h_q_tile;
+  std::vector<int> h_xh, h_xcov, h_unit_of, h_unit_pos, h_chunk_of, h_chunk_pos, h_u_cand, h_bpre;
+  std::vector<unsigned int> h_bmark;
+  std::vector<int64_t> h_u_off, h_xs_tile;
 };
 
 struct AddMap {                   // partner of each block of range A in range B (-1 = none)

@@ -595,7 +595,6 @@ UmmaPlan& get_umma_plan(System& S, int mult_type, int ra, int rb, int rc) {
   DevBuf<int> d_tc; d_tc.upload(tile_chunk, st);
   DevBuf<int> d_uc; d_uc.upload(u_cand.empty() ? std::vector<int>{0} : u_cand, st);
   DevBuf<int64_t> d_uoff; d_uoff.upload(u_off, st);
-  DevBuf<int64_t> d_xst; d_xst.upload(xs_tile, st);
   const int64_t mark_words = std::max<int64_t>(mark_total / 32, 1);
   const int64_t bkeys = (int64_t)n_units * n_chunks;
   const int64_t bwords = std::max<int64_t>((bkeys + 31) / 32, 1);
@@ -644,37 +643,73 @@ UmmaPlan& get_umma_plan(System& S, int mult_type, int ra, int rb, int rc) {
   U.units.alloc(std::max<int64_t>(uoff, 1), st);
   k_umma_units<<<(nt + 127) / 128, 128, 0, st>>>(nt, U.tiles.p, d_moff.p, d_mbits.p, d_mark.p, d_uc.p, d_uoff.p, d_tg.p,
                                                  d_tc.p, n_chunks, d_bmark.p, d_bpre.p, U.units.p);
-  // block tables of the slabs, and the per-slab row tables / units of the packing kernels
+  CQ_CUDA(cudaStreamSynchronize(st));
+  // what the slab tables need later (host copies; the device temporaries above are released now)
+  U.mult_type = mult_type; U.ra = ra; U.rb = rb; U.rc = rc;
+  U.n_groups = ng; U.n_chunks = n_chunks;
+  U.h_q_tile = std::move(q_tile); U.h_xh = std::move(xh); U.h_xcov = std::move(xcov);
+  U.h_unit_of = std::move(unit_of); U.h_unit_pos = std::move(unit_pos);
+  U.h_chunk_of = std::move(chunk_of); U.h_chunk_pos = std::move(chunk_pos);
+  U.h_u_cand = std::move(u_cand); U.h_u_off = std::move(u_off); U.h_xs_tile = std::move(xs_tile);
+  U.h_bmark = std::move(bm); U.h_bpre = std::move(bpre);
+  S.launches += 4;
+  auto res = S.uplans.emplace(key, std::move(up));
+  return *res.first->second;
+}
+
+// Slab tables and buffers of a tile plan, built on the product's first tensor-core call: the block of
+// every slab position (from the pair lists), the row tables and units of the packing kernels, and the
+// slab buffers themselves.
+static void umma_materialise(System& S, UmmaPlan& U) {
+  if (U.materialised) return;
+  cudaStream_t st = S.stream;
+  ProductPlan& P = get_plan(S, U.mult_type, U.ra, U.rb, U.rc);
+  RangeIndex& O = U.mult_type == 1 ? *S.ranges[U.rc] : *S.ranges[U.ra];
+  DevBuf<int2> d_qt; d_qt.upload(U.h_q_tile, st);
+  DevBuf<int> d_xh; d_xh.upload(U.h_xh, st);
+  DevBuf<int> d_xcov; d_xcov.upload(U.h_xcov, st);
+  DevBuf<int> d_uof; d_uof.upload(U.h_unit_of, st);
+  DevBuf<int> d_upos; d_upos.upload(U.h_unit_pos, st);
+  DevBuf<int> d_chof; d_chof.upload(U.h_chunk_of, st);
+  DevBuf<int> d_chpos; d_chpos.upload(U.h_chunk_pos, st);
+  DevBuf<unsigned int> d_bmark; d_bmark.upload(U.h_bmark, st);
+  DevBuf<int> d_bpre; d_bpre.upload(U.h_bpre, st);
+  DevBuf<int64_t> d_xst; d_xst.upload(U.h_xs_tile, st);
+  PlanDev D;
+  D.ptr = P.ptr.p; D.pairs = P.pairs.p; D.q_tile = d_qt.p; D.xh = d_xh.p; D.xcov = d_xcov.p; D.ocov = O.nb_cover.p;
+  D.unit_of = d_uof.p; D.unit_pos = d_upos.p; D.chunk_of = d_chof.p; D.chunk_pos = d_chpos.p; D.mark_off = nullptr;
+  D.n_chunks = U.n_chunks;
   const int64_t tabw = kMaxUnitAtoms * kMaxAtoms;
   U.xtab.alloc(std::max<int64_t>(U.n_xslabs, 1) * tabw, st);
-  U.btab.alloc(std::max<int64_t>(n_bslabs, 1) * tabw, st);
+  U.btab.alloc(std::max<int64_t>(U.n_bslabs, 1) * tabw, st);
   CQ_CUDA(cudaMemsetAsync(U.xtab.p, 0xff, sizeof(int) * U.xtab.n, st));
   CQ_CUDA(cudaMemsetAsync(U.btab.p, 0xff, sizeof(int) * U.btab.n, st));
-  k_umma_btab<<<gw, T256, 0, st>>>(n_out, D, d_bmark.p, d_bpre.p, d_xst.p, U.xtab.p, U.btab.p);
+  const int n_out = O.nnz;
+  const int gw = (int)(((int64_t)n_out * 32 + 255) / 256);
+  k_umma_btab<<<gw, 256, 0, st>>>(n_out, D, d_bmark.p, d_bpre.p, d_xst.p, U.xtab.p, U.btab.p);
   CQ_CUDA(cudaGetLastError());
   std::vector<int> xs_rtab(std::max<int64_t>(U.n_xslabs, 1), 0), xs_unit(std::max<int64_t>(U.n_xslabs, 1), 0);
-  for (int gi = 0; gi < ng; ++gi)
-    for (int64_t h = u_off[gi]; h < u_off[gi + 1]; ++h) { xs_rtab[h] = gi * kM; xs_unit[h] = u_cand[h]; }
+  for (int gi = 0; gi < U.n_groups; ++gi)
+    for (int64_t h = U.h_u_off[gi]; h < U.h_u_off[gi + 1]; ++h) { xs_rtab[h] = gi * kM; xs_unit[h] = U.h_u_cand[h]; }
   U.xs_rtab.upload(xs_rtab, st);
   U.xs_unit.upload(xs_unit, st);
-  // B slabs in key order (key = unit * n_chunks + chunk), as ranked above
+  // B slabs in key order (key = unit * n_chunks + chunk), as ranked by the plan
   std::vector<int> bs_rtab, bs_unit;
-  bs_rtab.reserve(std::max<int64_t>(n_bslabs, 1)); bs_unit.reserve(std::max<int64_t>(n_bslabs, 1));
-  for (int64_t w = 0; w < bwords; ++w)
-    for (unsigned int m = bm[w]; m; m &= m - 1) {
-      const int64_t k = 32 * w + __builtin_ctz(m);
-      bs_unit.push_back((int)(k / n_chunks));
-      bs_rtab.push_back((int)((ng + k % n_chunks) * kM));
+  bs_rtab.reserve(std::max<int64_t>(U.n_bslabs, 1)); bs_unit.reserve(std::max<int64_t>(U.n_bslabs, 1));
+  for (size_t w = 0; w < U.h_bmark.size(); ++w)
+    for (unsigned int m = U.h_bmark[w]; m; m &= m - 1) {
+      const int64_t k = 32 * (int64_t)w + __builtin_ctz(m);
+      bs_unit.push_back((int)(k / U.n_chunks));
+      bs_rtab.push_back((int)((U.n_groups + k % U.n_chunks) * kM));
     }
   if (bs_rtab.empty()) { bs_rtab.push_back(0); bs_unit.push_back(0); }
   U.bs_rtab.upload(bs_rtab, st);
   U.bs_unit.upload(bs_unit, st);
   U.xslabs.alloc((size_t)std::max<int64_t>(U.n_xslabs, 1) * (kSlabBytes / 16), st);
-  U.bslabs.alloc((size_t)std::max<int64_t>(n_bslabs, 1) * (kSlabBytes / 16), st);
+  U.bslabs.alloc((size_t)std::max<int64_t>(U.n_bslabs, 1) * (kSlabBytes / 16), st);
   CQ_CUDA(cudaStreamSynchronize(st));
-  S.launches += 5;
-  auto res = S.uplans.emplace(key, std::move(up));
-  return *res.first->second;
+  S.launches += 1;
+  U.materialised = true;
 }
 
 static int* umma_err_word(System& S) {
@@ -694,6 +729,7 @@ void mat_mult_umma(System& S, int mult_type, int ra, int rb, int rc, double* a, 
   UmmaPlan& U = get_umma_plan(S, mult_type, ra, rb, rc);
   CQ_CHECK(U.usable, CQ_ERR_ARG, "tensor-core tiles need block sizes of 4 to 16");
   if (U.n_tiles == 0) return;
+  umma_materialise(S, U);
   RangeIndex &A = *S.ranges[ra], &B = *S.ranges[rb], &C = *S.ranges[rc];
   RangeIndex& O = mult_type == 1 ? C : A;
   RangeIndex& X = mult_type == 1 ? A : C;

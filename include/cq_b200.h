@@ -213,6 +213,19 @@ int cq_m_kern_min(int k_off, int kpart, const int* ib_nd_acc, const int* ibaddr,
                   int chalo_ni_in_halo, const int* at_i_prim, const int* at_i_beg, const int* at_i_nd_beg,
                   const int* at_n_hnab, int mx_absb, int mx_part, int mx_iprim, int lena, int lenb, int lenc);
 
+/* Deferred drop-in calls (no counterpart in the reference, whose kernels return with their result in
+ * c): with np_in_halo > 0 (the A halo's partition count, ahalo%np_in_halo, which the Fortran shim
+ * passes before every m_kern call) the cq_m_kern_max / cq_m_kern_min calls of one mat_mult partition
+ * loop keep a and c on the device from the first partition (kpart == 1) on, copy only their
+ * partition's b and block lists, enqueue their arithmetic and return; the call with
+ * kpart == np_in_halo copies the result (c for m_kern_max, a for m_kern_min) back to the array the
+ * first partition's call passed and synchronises.  a and c must not change between the calls of
+ * one loop (mat_mult does not change them).  cq_m_kern_flush completes an open loop at once;
+ * cq_m_kern_defer(0) flushes and returns to complete-per-call.  Per calling thread.  Results are
+ * bit-identical to complete-per-call. */
+int cq_m_kern_defer(int np_in_halo);
+int cq_m_kern_flush(void);
+
 /* matrix_sum (src/mult_module.f90:2677-2715): a = alpha*a + beta*b; ranges may differ (matrix_add rules). */
 int cq_matrix_sum(cq_system* sys, int ra, double* a_dev, double alpha, int rb, const double* b_dev, double beta);
 /* matrix_transpose within one range (src/mult_module.f90:2609-2673). */

@@ -33,7 +33,9 @@ def _loc_trans(o, r, a, atrans, invdir):
             tpos += nd1 * nd2
 
 
-def mat_mult_dropin(o, mult_type, ra, rb, rc, a, b, c):
+def mat_mult_dropin(o, mult_type, ra, rb, rc, a, b, c, deferred=False):
+    """deferred: the shim passes ahalo%np_in_halo before every call (cq_m_kern_defer), so the loop's calls
+    enqueue their work and the last partition's call completes it."""
     cd = o.geti("cover_dims")
     ncy, ncz = int(cd[1]), int(cd[2])
     ngnode = o.geti("ngnode")
@@ -86,7 +88,11 @@ def mat_mult_dropin(o, mult_type, ra, rb, rc, a, b, c):
                 ibpart[ibind[k] + ni - 1] = npxyz[noff + 3 * ni] * ncy * ncz + npxyz[noff + 3 * ni + 1] * ncz + npxyz[noff + 3 * ni + 2]
             noff += 3 * nbnab[k]
         k_off = int(lab_hcover[kpart - 1])
+        if deferred:
+            cq_b200.m_kern_defer(len(lab_hcell))
         cq_b200.m_kern("max" if mult_type == 1 else "min", k_off, kpart, ib_nd_acc, ibind, nbnab, ibpart, ibseq, bndim2,
                        atrans, b_rem, c, ah, ch, at)
+    if deferred:
+        cq_b200.m_kern_defer(0)
     if mult_type == 2:
         _loc_trans(o, ra, a, atrans, 1)

@@ -157,9 +157,11 @@ def test_lnv_products_sz_bit_exact(cfg2, prod, variant):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("deferred", [False, True])
 @pytest.mark.parametrize("mult_type", [1, 2])
-def test_dropin_kernels_match_default(cfg2, mult_type):
-    """mat_mult's partition loop calling cq_m_kern_max / cq_m_kern_min reproduces the default kernel."""
+def test_dropin_kernels_match_default(cfg2, mult_type, deferred):
+    """mat_mult's partition loop calling cq_m_kern_max / cq_m_kern_min reproduces the default kernel,
+    completing every call or (deferred) enqueuing the loop's calls and completing at the last partition."""
     o, g, bls, idx = cfg2
     ra, rb, rc = ("L", "S", "LS") if mult_type == 1 else ("L", "LS", "SLS")
     ia, ib, ic = idx[ra], idx[rb], idx[rc]
@@ -168,10 +170,10 @@ def test_dropin_kernels_match_default(cfg2, mult_type):
     c = inputs.random_blocks(bls[rc], 32, inputs.TAG_RANDOM_A)
     if mult_type == 1:
         ref = np.zeros(bls[rc].length); o.mat_mult(1, ia, ib, ic, a, b, ref)
-        got = np.zeros(bls[rc].length); dropin_driver.mat_mult_dropin(o, 1, ia, ib, ic, a, b, got)
+        got = np.zeros(bls[rc].length); dropin_driver.mat_mult_dropin(o, 1, ia, ib, ic, a, b, got, deferred)
     else:
         ref = np.zeros(bls[ra].length); o.mat_mult(2, ia, ib, ic, ref, b, c)
-        got = np.zeros(bls[ra].length); dropin_driver.mat_mult_dropin(o, 2, ia, ib, ic, got, b, c)
+        got = np.zeros(bls[ra].length); dropin_driver.mat_mult_dropin(o, 2, ia, ib, ic, got, b, c, deferred)
     assert np.array_equal(got, ref)
 
 
