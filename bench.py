@@ -362,6 +362,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mixed-sample-only", action="store_true",
+                    help="run only the mixed-precision vs FP64 comparison on the DZP sample (with --tol, --max-outer)")
     ap.add_argument("--no-mixed-sample", action="store_true",
                     help="skip the mixed-precision vs FP64 comparison on the bounded DZP sample")
     ap.add_argument("--workload", default="lnv512", choices=["lnv512", "batch", "serve", "mult216", "mult512", "mult4096"],
@@ -399,6 +401,12 @@ def main():
         return
     if args.impl == "reference":
         return reference_main(args, ws, rank)
+    if args.mixed_sample_only:
+        import torch
+        import cq_b200
+        torch.cuda.set_device(local)
+        emit({"mixed_vs_fp64": mixed_vs_fp64(cq_b200, args.tol, args.max_outer)})
+        return
     if args.cpu_full_solve:
         if rank == 0:
             cpu_full_solve(args.cpu_full_solve)
@@ -608,37 +616,49 @@ def run_server(cq_b200, reqs, n_slots, mixed, rate=None, seed=0):
 
 
 def mixed_sample_requests():
-    """Bounded DZP sample of the mixed-precision comparison in the default bench line: two Si clusters
-    (64 and 100 atoms) and two periodic supercells (64 atoms, sigma 0.1 bohr, different seeds), 13x13
-    blocks, 2 electrons per atom, ranges as the 512-atom workload, per-request generator seeds."""
+    """Bounded DZP sample of the mixed-precision comparison in the default bench line: four periodic Si
+    supercells of 64 atoms (2x2x2 cells, sigma 0.1 bohr, different seeds), 13x13 blocks, 2 electrons per
+    atom, ranges as the 512-atom workload, per-request generator seeds."""
     from cq_b200 import inputs
     out = []
-    for k, (kind, n) in enumerate((("cluster", 64), ("cell", 2), ("cluster", 100), ("cell", 2))):
-        if kind == "cluster":
-            c, cell = inputs.si_cluster(n, sigma=0.1, seed=2000 + k)
-        else:
-            c, cell = inputs.diamond_si(n, sigma=0.1, seed=2000 + k)
+    for k in range(4):
+        c, cell = inputs.diamond_si(2, sigma=0.1, seed=2000 + k)
         out.append(dict(coords=c, cell=cell, nsf=13, ne=2.0 * len(c), seed=6000 + k, n=len(c)))
     return out
 
 
-def mixed_vs_fp64(cq_b200):
+MIXED_SAMPLE_TOL = 1e-8    # residual at which both arms of the mixed-precision comparison stop
+MIXED_SAMPLE_MAX_OUTER = 12
+
+
+def mixed_vs_fp64(cq_b200, tol=None, max_outer=None):
     """The precision form against the plain FP64 path on the bounded DZP sample: FP64 solves one at a
-    time, mixed-precision solves on 4 concurrent slots; both stop at residual SERVE_TOL (pass limit
-    SERVE_MAX_OUTER).  Solves/s of both arms, their ratio and the largest |dE| per atom."""
-    reqs = mixed_sample_requests()
-    fp, t_fp = run_server(cq_b200, reqs, 1, False)
-    mx, t_mx = run_server(cq_b200, reqs, 4, True)
-    ok = [(a, b) for a, b in zip(fp, mx) if a["status"] == 0 and b["status"] == 0]
-    err = max([abs(a["energy"] - b["energy"]) / a["n_atoms"] for a, b in ok], default=None)
-    return {"sample": "4 DZP (13x13) Si systems: clusters of 64 and 100 atoms, two 64-atom supercells; S/H/L/T "
-                      "10/12/16/10 bohr; both arms stop at residual %g (pass limit %d)" % (SERVE_TOL, SERVE_MAX_OUTER),
+    time, mixed-precision solves on 4 concurrent slots; both stop at residual `tol` (pass limit
+    `max_outer`).  Solves/s of both arms, their ratio, and |dE| per atom of every request."""
+    global SERVE_TOL, SERVE_MAX_OUTER
+    saved = (SERVE_TOL, SERVE_MAX_OUTER)
+    SERVE_TOL = MIXED_SAMPLE_TOL if tol is None else tol
+    SERVE_MAX_OUTER = MIXED_SAMPLE_MAX_OUTER if max_outer is None else max_outer
+    try:
+        reqs = mixed_sample_requests()
+        fp, t_fp = run_server(cq_b200, reqs, 1, False)
+        mx, t_mx = run_server(cq_b200, reqs, 4, True)
+        tol_used, mo_used = SERVE_TOL, SERVE_MAX_OUTER
+    finally:
+        SERVE_TOL, SERVE_MAX_OUTER = saved
+    per = [{"n": a["n_atoms"], "fp64_converged": int(a["converged"]), "mixed_converged": int(b["converged"]),
+            "dE_per_atom_Ha": (b["energy"] - a["energy"]) / a["n_atoms"], "fp64_s": a["t_done"] - a["t_admit"],
+            "mixed_s": b["t_done"] - b["t_admit"]} for a, b in zip(fp, mx) if a["status"] == 0 and b["status"] == 0]
+    both = [abs(r["dE_per_atom_Ha"]) for r in per if r["fp64_converged"] and r["mixed_converged"]]
+    return {"sample": "4 periodic DZP (13x13) Si supercells of 64 atoms; S/H/L/T 10/12/16/10 bohr; both arms stop at "
+                      "residual %g (pass limit %d)" % (tol_used, mo_used),
             "fp64": {"solves_per_s": len(reqs) / t_fp, "seconds": t_fp, "slots": 1},
             "mixed": {"solves_per_s": len(reqs) / t_mx, "seconds": t_mx, "slots": 4,
                       "precision": "bf16x3 split products (tensor cores), FP64 traces, line search, Hotelling, "
                                    "McWeeny start and FP64 continuation from residual 1e-6"},
-            "ratio": t_fp / t_mx, "max_abs_dE_per_atom_Ha": err,
-            "converged": [int(a["converged"]) for a in fp] + [int(b["converged"]) for b in mx],
+            "ratio": t_fp / t_mx,
+            "max_abs_dE_per_atom_Ha_converged": max(both) if both else None,
+            "per_request": per,
             "failed": sum(1 for r in fp + mx if r["status"] != 0),
             "target": "mixed >= 5x the FP64 solves/s at <= 1e-8 Ha/atom"}
 

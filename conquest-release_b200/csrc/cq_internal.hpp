@@ -251,6 +251,7 @@ struct UmmaPlan {
   DevBuf<unsigned int> rtabs, ktabs;   // row tables (row groups, column chunks); K tables of the units
   DevBuf<int> outmap, xtab, btab, xs_rtab, xs_unit, bs_rtab, bs_unit;
   DevBuf<uint4> xslabs, bslabs;   // packed bf16 operands, 8 KB per slab, rewritten by every product call
+  DevBuf<int> tile_counter;       // the persistent kernel's next tile
   // host side of the plan, kept to build the slab tables and buffers on the product's first
   // tensor-core call (a product that runs on the per-block kernel never allocates them)
   bool materialised = false;

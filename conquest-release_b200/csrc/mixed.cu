@@ -254,9 +254,10 @@ static void mat_mult_mma_sync(System& S, MixedPlan& MP, int mult_type, int ra, i
 // the product's tile plan, so that a product always runs the same kernel (and gives the same bits)
 // whatever else runs on the device: the tcgen05 tiles where at least kTileMinFill of their issued
 // tensor work is useful (3 x the product's flops / issued flops), else the per-block mma.sync kernel.
-// Measured on B200: the tiles issue 300-800 TFLOP/s and the per-block kernel about 170 at a useful
-// fraction near 0.5, so the tiles pay above roughly 0.15.
-constexpr double kTileMinFill = 0.15;
+// Measured on B200 (4096-atom DZP cell, the nine products of an LNV call): the tiles issue 330-850
+// TFLOP/s at useful fractions of 0.056-0.114 and the per-block kernel reaches 25-31 TFLOP/s useful;
+// the tiles were faster for the product with fraction 0.114 (31.1 against 29.3) and slower below.
+constexpr double kTileMinFill = 0.11;
 
 void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c) {
   MixedPlan& MP = get_mixed_plan(S, mult_type, ra, rb, rc);

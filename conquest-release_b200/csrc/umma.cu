@@ -15,12 +15,14 @@
 // (row group, unit) holds the first operand's 128 rows x 16 K, a B slab per (unit, column chunk)
 // the second operand's 128 columns x 16 K, each as a hi part (bf16(v)) and a lo part (bf16(v - hi)),
 // about 16 significant bits; absent blocks are zeros.
-// The product kernel is one CTA per tile.  One thread moves the slabs of each pipeline stage into
-// shared memory with cp.async.bulk (no multicast; 16 KB per unit, completion counted on an mbarrier),
-// one thread issues per unit the three MMAs lo.hi + hi.lo + hi.hi (kind::f16, bf16 inputs, FP32
-// accumulation) into a 128 x 128 FP32 accumulator in tensor memory, a tcgen05.commit per stage frees
-// it, and four warps read the accumulator back with tcgen05.ld and write every stored output block of
-// the tile as FP64 (the whole block is overwritten, as the FP64 kernels do).  Pairs absent from the
+// The product kernel is persistent, two CTAs per SM each walking its share of the tiles.  One thread moves
+// the slabs of each pipeline stage into shared memory with cp.async.bulk (no multicast; 16 KB per unit,
+// completion counted on an mbarrier), in one ring of three stages across the CTA's tiles; one thread
+// issues per unit the three MMAs lo.hi + hi.lo + hi.hi (kind::f16, bf16 inputs, FP32 accumulation)
+// into a 128 x 128 FP32 accumulator in tensor memory, a tcgen05.commit per stage frees it; the tiles
+// alternate between two accumulators, so that while the MMAs of one tile run, four warps read the
+// previous tile's accumulator back with tcgen05.ld and write every stored output block of it as FP64
+// (the whole block is overwritten, as the FP64 kernels do).  Pairs absent from the
 // pair lists contribute zero blocks, so a tile computes exactly the sums over the (i, k, j) triples of
 // the reference kernel, in a different order and precision.
 //
@@ -46,7 +48,7 @@ constexpr int kStages = 3;
 constexpr int kMaxAtoms = 32;       // atoms per row group / column chunk (block sizes >= 4)
 constexpr int kMaxUnitAtoms = 4;
 constexpr int kMinNd = 4;
-constexpr uint32_t kTmemCols = kNT;
+constexpr uint32_t kTmemCols = 2 * kNT;   // two accumulators: one tile's epilogue overlaps the next one's MMAs
 constexpr int kThreads = 192;       // warps 0-3 epilogue, warp 4 bulk copies, warp 5 TMEM + MMA
 
 // one slab: hi part then lo part, each [K group (2)][row group (16)][8 rows x 16 bytes]
@@ -59,14 +61,15 @@ constexpr int kStageBytes = 4 * kRegion;
 
 struct Smem {
   alignas(1024) unsigned char stage[kStages][kStageBytes];
-  unsigned int rowtab[kM];          // row m -> ii | n1 << 8 | nd << 16 (0xffffffff: unused row)
-  unsigned int coltab[kNT];         // column -> jj | nn << 8 | nd << 16
-  unsigned long long full[kStages], empty[kStages], accfull;
+  unsigned int coltab[kNT];         // column -> jj | nn << 8 | nd << 16 of the epilogue's current tile
+  unsigned long long full[kStages], empty[kStages];
+  unsigned long long acc_full[2], acc_empty[2], drain;
+  unsigned long long tile_full[4], tile_empty[4];   // ring of the CTA's next tiles (fetched dynamically)
+  int tile_ring[4];
   unsigned int tmem_base;
   int abort;
 };
-// two CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA): one CTA's set-up and epilogue
-// overlap the other's MMAs; their two 128-column accumulators fit the 512 TMEM columns
+// two persistent CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA; 2 x 256 TMEM columns)
 static_assert(sizeof(Smem) + 1024 <= 113 * 1024, "shared memory of the tensor-core product exceeds half an SM");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -79,6 +82,9 @@ __device__ __forceinline__ uint64_t global_ns() {
 
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
@@ -118,6 +124,20 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                    smem_u32(dst)),
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
+}
+
+// named barrier of the four epilogue warps that also ORs a flag over them
+__device__ __forceinline__ bool epilogue_any(bool flag) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.b32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)flag)
+      : "memory");
+  return r != 0;
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -236,19 +256,27 @@ struct UmmaArgs {
   const int64_t* __restrict__ o_elem;
   double* __restrict__ out;
   int* err;                           // mapped host word: a bounded wait ran out
+  int* tile_counter;                  // next tile to take (zeroed before the launch)
 };
 
-__global__ void __launch_bounds__(kThreads, 2) k_mult_umma(UmmaArgs P) {
+// Persistent: the bulk-copy thread of each CTA takes the next tile from a device-wide counter when it
+// is ready for one (long and short tiles balance over the CTAs) and passes its number to the MMA
+// thread and the epilogue warps through a four-entry ring in shared memory.  The bulk-copy thread and
+// the MMA thread walk one continuous ring of stages across the CTA's tiles; tile number c of the CTA
+// accumulates in TMEM buffer c % 2, which the epilogue warps read back (and release) while the MMAs
+// of tile c + 1 run in the other buffer.
+__global__ void __launch_bounds__(kThreads, 2) k_mult_umma(UmmaArgs P, int n_tiles) {
   extern __shared__ unsigned char smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const UmmaTile T = P.tiles[blockIdx.x];
-  const int nstage = (T.n_u + kUnitsPerStage - 1) / kUnitsPerStage;
 
-  // ---- set-up: barriers, TMEM, row and column tables of the tile
+  // ---- set-up: barriers and TMEM
   if (tid == 128) {
     for (int s = 0; s < kStages; ++s) { mbar_init(&sm.full[s], 1); mbar_init(&sm.empty[s], 1); }
-    mbar_init(&sm.accfull, 1);
+    for (int b = 0; b < 2; ++b) { mbar_init(&sm.acc_full[b], 1); mbar_init(&sm.acc_empty[b], 128); }
+    // a ring entry is read by the MMA thread and by the four epilogue warps before it is reused
+    for (int q = 0; q < 4; ++q) { mbar_init(&sm.tile_full[q], 1); mbar_init(&sm.tile_empty[q], 5); }
+    mbar_init(&sm.drain, 1);
     sm.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -258,8 +286,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_mult_umma(UmmaArgs P) {
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (tid < kM) sm.rowtab[tid] = P.rtabs[T.row_tab + tid];
-  for (int n = tid; n < kNT; n += kThreads) sm.coltab[n] = P.rtabs[T.col_tab + n];
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -267,92 +293,144 @@ __global__ void __launch_bounds__(kThreads, 2) k_mult_umma(UmmaArgs P) {
 
   if (warp == 4) {
     if (lane == 0) {
-      // ---- bulk copies: the X and B slabs of each stage's units
-      for (int c = 0; c < nstage; ++c) {
-        const int s = c % kStages;
-        if (c >= kStages && !mbar_wait(&sm.empty[s], ((c / kStages) - 1) & 1, P.err, &sm.abort)) break;
-        const int u0 = c * kUnitsPerStage, nu = min(kUnitsPerStage, T.n_u - u0);
-        mbar_expect_tx(&sm.full[s], (uint32_t)(nu * 2 * kSlabBytes));
-        unsigned char* st = sm.stage[s];
-        for (int u = 0; u < nu; ++u) {
-          const int2 e = P.units[T.u_off + u0 + u];
-          const unsigned char* xs = reinterpret_cast<const unsigned char*>(P.xslabs) + (size_t)e.x * kSlabBytes;
-          const unsigned char* bs = reinterpret_cast<const unsigned char*>(P.bslabs) + (size_t)e.y * kSlabBytes;
-          bulk_g2s(st + 0 * kRegion + u * kSlabHalf, xs, kSlabHalf, &sm.full[s]);
-          bulk_g2s(st + 1 * kRegion + u * kSlabHalf, xs + kSlabHalf, kSlabHalf, &sm.full[s]);
-          bulk_g2s(st + 2 * kRegion + u * kSlabHalf, bs, kSlabHalf, &sm.full[s]);
-          bulk_g2s(st + 3 * kRegion + u * kSlabHalf, bs + kSlabHalf, kSlabHalf, &sm.full[s]);
+      // ---- bulk copies: the X and B slabs of each stage's units, tile after tile
+      uint32_t it = 0;                 // stages issued by this CTA
+      bool ok = true;
+      for (uint32_t q = 0; ok; ++q) {
+        // the next tile of the product: taken from a device-wide counter, published in the ring
+        const int slot = q & 3;
+        if (q >= 4 && !mbar_wait(&sm.tile_empty[slot], ((q >> 2) - 1) & 1, P.err, &sm.abort)) { ok = false; break; }
+        const int t = atomicAdd(P.tile_counter, 1);
+        sm.tile_ring[slot] = t < n_tiles ? t : -1;
+        mbar_arrive(&sm.tile_full[slot]);
+        if (t >= n_tiles) break;
+        const UmmaTile T = P.tiles[t];
+        for (int u0 = 0; u0 < T.n_u; u0 += kUnitsPerStage, ++it) {
+          const int s = it % kStages;
+          if (it >= kStages && !mbar_wait(&sm.empty[s], ((it / kStages) - 1) & 1, P.err, &sm.abort)) { ok = false; break; }
+          const int nu = min(kUnitsPerStage, T.n_u - u0);
+          mbar_expect_tx(&sm.full[s], (uint32_t)(nu * 2 * kSlabBytes));
+          unsigned char* st = sm.stage[s];
+          for (int u = 0; u < nu; ++u) {
+            const int2 e = P.units[T.u_off + u0 + u];
+            const unsigned char* xs = reinterpret_cast<const unsigned char*>(P.xslabs) + (size_t)e.x * kSlabBytes;
+            const unsigned char* bs = reinterpret_cast<const unsigned char*>(P.bslabs) + (size_t)e.y * kSlabBytes;
+            bulk_g2s(st + 0 * kRegion + u * kSlabHalf, xs, kSlabHalf, &sm.full[s]);
+            bulk_g2s(st + 1 * kRegion + u * kSlabHalf, xs + kSlabHalf, kSlabHalf, &sm.full[s]);
+            bulk_g2s(st + 2 * kRegion + u * kSlabHalf, bs, kSlabHalf, &sm.full[s]);
+            bulk_g2s(st + 3 * kRegion + u * kSlabHalf, bs + kSlabHalf, kSlabHalf, &sm.full[s]);
+          }
         }
+      }
+      if (!ok) {
+        // copies still in flight land in shared memory: wait for the stages issued last (bounded)
+        int dummy = 0;
+        for (uint32_t k = it > kStages ? it - kStages : 0; k < it; ++k)
+          mbar_wait(&sm.full[k % kStages], (k / kStages) & 1, P.err, &dummy);
       }
     }
   } else if (warp == 5) {
     if (lane == 0) {
       // ---- MMA issue (one thread)
       constexpr uint32_t idesc = idesc_bf16(kM, kNT);
-      for (int c = 0; c < nstage; ++c) {
-        const int s = c % kStages;
-        if (!mbar_wait(&sm.full[s], (c / kStages) & 1, P.err, &sm.abort)) break;
+      uint32_t it = 0, tc = 0;         // stages consumed, tiles accumulated by this CTA
+      bool ok = true;
+      for (uint32_t q = 0; ok; ++q, ++tc) {
+        const int slot = q & 3;
+        if (!mbar_wait(&sm.tile_full[slot], (q >> 2) & 1, P.err, &sm.abort)) { ok = false; break; }
+        const int t = *(volatile int*)&sm.tile_ring[slot];
+        mbar_arrive(&sm.tile_empty[slot]);
+        if (t < 0) break;
+        const int n_u = P.tiles[t].n_u;
+        const int b = tc & 1;
+        if (tc >= 2 && !mbar_wait(&sm.acc_empty[b], ((tc >> 1) - 1) & 1, P.err, &sm.abort)) { ok = false; break; }
         tc_fence_after();
-        const uint32_t base = smem_u32(sm.stage[s]);
-        const int nu = min(kUnitsPerStage, T.n_u - c * kUnitsPerStage);
-        for (int u = 0; u < nu; ++u) {
-          const uint32_t o = u * kSlabHalf;
-          const uint64_t dah = smem_desc(base + 0 * kRegion + o, 2048, 128);
-          const uint64_t dal = smem_desc(base + 1 * kRegion + o, 2048, 128);
-          const uint64_t dbh = smem_desc(base + 2 * kRegion + o, 2048, 128);
-          const uint64_t dbl = smem_desc(base + 3 * kRegion + o, 2048, 128);
-          umma_bf16(tmem, dal, dbh, idesc, (c > 0 || u > 0) ? 1u : 0u);
-          umma_bf16(tmem, dah, dbl, idesc, 1u);
-          umma_bf16(tmem, dah, dbh, idesc, 1u);
+        const uint32_t acc = tmem + b * kNT;
+        for (int u0 = 0; u0 < n_u; u0 += kUnitsPerStage, ++it) {
+          const int s = it % kStages;
+          if (!mbar_wait(&sm.full[s], (it / kStages) & 1, P.err, &sm.abort)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t base = smem_u32(sm.stage[s]);
+          const int nu = min(kUnitsPerStage, n_u - u0);
+          for (int u = 0; u < nu; ++u) {
+            const uint32_t o = u * kSlabHalf;
+            const uint64_t dah = smem_desc(base + 0 * kRegion + o, 2048, 128);
+            const uint64_t dal = smem_desc(base + 1 * kRegion + o, 2048, 128);
+            const uint64_t dbh = smem_desc(base + 2 * kRegion + o, 2048, 128);
+            const uint64_t dbl = smem_desc(base + 3 * kRegion + o, 2048, 128);
+            umma_bf16(acc, dal, dbh, idesc, (u0 > 0 || u > 0) ? 1u : 0u);
+            umma_bf16(acc, dah, dbl, idesc, 1u);
+            umma_bf16(acc, dah, dbh, idesc, 1u);
+          }
+          umma_commit(&sm.empty[s]);
         }
-        umma_commit(&sm.empty[s]);
+        if (ok) umma_commit(&sm.acc_full[b]);   // the tile's accumulator is complete (empty tiles too)
       }
-      // completion of every MMA issued above (also on the error path, before TMEM is released)
-      umma_commit(&sm.accfull);
+      // every MMA issued above has completed before the tensor memory can be released
+      umma_commit(&sm.drain);
+      int dummy = 0;
+      mbar_wait(&sm.drain, 0, P.err, &dummy, 2000000000ull);
     }
   } else {
-    // ---- epilogue (warps 0-3, TMEM lane quarter = warp): accumulator -> FP64 output blocks
-    bool have = nstage > 0 && mbar_wait(&sm.accfull, 0, P.err, &sm.abort, 2000000000ull);
-    have = __all_sync(0xffffffffu, have && !*(volatile int*)&sm.abort);   // tcgen05.ld is warp-wide
-    tc_fence_after();
+    // ---- epilogue (warps 0-3, TMEM lane quarter = warp): accumulators -> FP64 output blocks
     const int m = warp * 32 + lane;
-    const unsigned int ri = sm.rowtab[m];
-    for (int cb = 0; cb < kNT / 16; ++cb) {
-      uint32_t r[16];
-      if (have) tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + cb * 16, r);
-      else {
-#pragma unroll
-        for (int e = 0; e < 16; ++e) r[e] = 0u;
-      }
-      if (ri == 0xffffffffu) continue;
+    uint32_t tc = 0;
+    for (uint32_t q = 0;; ++q, ++tc) {
+      const int slot = q & 3;
+      const bool got = mbar_wait(&sm.tile_full[slot], (q >> 2) & 1, P.err, &sm.abort);
+      const int t = got ? *(volatile int*)&sm.tile_ring[slot] : -1;
+      __syncwarp();
+      if (lane == 0 && got) mbar_arrive(&sm.tile_empty[slot]);
+      if (epilogue_any(!got)) break;   // uniform over the epilogue warps (a wait ran out: aborted)
+      if (t < 0) break;                // the same ring entry for every epilogue thread: uniform
+      const UmmaTile T = P.tiles[t];
+      const int b = tc & 1;
+      const bool ok = mbar_wait(&sm.acc_full[b], (tc >> 1) & 1, P.err, &sm.abort, 2000000000ull);
+      // the column table of this tile (the previous tile's users have passed the barrier at the end)
+      sm.coltab[m] = P.rtabs[T.col_tab + m];
+      if (epilogue_any(!ok)) break;    // a barrier of the four epilogue warps: the decision is uniform
+      tc_fence_after();
+      const unsigned int ri = P.rtabs[T.row_tab + m];
       const int ii = ri & 0xff, n1 = (ri >> 8) & 0xff, ndi = ri >> 16;
-      int jj_prev = -1;
-      long long base = -1;
+      // two halves of 64 columns; the buffer is released once the second half has been read
+#pragma unroll 1
+      for (int half = 0; half < 2; ++half) {
+        uint32_t r[4][16];
 #pragma unroll
-      for (int e = 0; e < 16; ++e) {
-        const unsigned int ci = sm.coltab[cb * 16 + e];
-        if (ci == 0xffffffffu) continue;
-        const int jj = ci & 0xff, nn = (ci >> 8) & 0xff;
-        if (jj != jj_prev) {
-          const int q = __ldg(P.outmap + T.om_off + ii * T.n_cols + jj);
-          base = q >= 0 ? (long long)P.o_elem[q] : -1ll;
-          jj_prev = jj;
+        for (int cb = 0; cb < 4; ++cb) {
+          if (T.n_u > 0) tmem_ld16(tmem + b * kNT + ((uint32_t)(warp * 32) << 16) + (half * 4 + cb) * 16, r[cb]);
+          else {
+#pragma unroll
+            for (int e = 0; e < 16; ++e) r[cb][e] = 0u;
+          }
         }
-        if (base >= 0) P.out[base + n1 + (int64_t)ndi * nn] = (double)__uint_as_float(r[e]);
+        if (half == 1) {
+          tc_fence_before();
+          mbar_arrive(&sm.acc_empty[b]);   // the MMAs of tile c + 2 may overwrite this buffer now
+        }
+        if (ri == 0xffffffffu) continue;
+        int jj_prev = -1;
+        long long base = -1;
+#pragma unroll
+        for (int e = 0; e < 64; ++e) {
+          const unsigned int ci = sm.coltab[half * 64 + e];
+          if (ci == 0xffffffffu) continue;
+          const int jj = ci & 0xff, nn = (ci >> 8) & 0xff;
+          if (jj != jj_prev) {
+            const int q = __ldg(P.outmap + T.om_off + ii * T.n_cols + jj);
+            base = q >= 0 ? (long long)P.o_elem[q] : -1ll;
+            jj_prev = jj;
+          }
+          if (base >= 0) P.out[base + n1 + (int64_t)ndi * nn] = (double)__uint_as_float(r[e >> 4][e & 15]);
+        }
       }
+      asm volatile("bar.sync 2, 128;" ::: "memory");
     }
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 5) {
     tc_fence_after();
-    // after an aborted pipeline the epilogue may not have seen the copies and MMAs complete: wait for
-    // them (bounded) before the tensor memory and the shared memory are released
-    if (nstage > 0 && *(volatile int*)&sm.abort) {
-      int dummy = 0;
-      if (lane == 0) mbar_wait(&sm.accfull, 0, P.err, &dummy, 2000000000ull);
-      __syncwarp();
-    }
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
   }
 }
@@ -757,9 +835,15 @@ void mat_mult_umma(System& S, int mult_type, int ra, int rb, int rc, double* a, 
   M.o_elem = O.nb_elem.p;
   M.out = mult_type == 1 ? c : a;
   M.err = umma_err_word(S);
+  if (!U.tile_counter.n) U.tile_counter.alloc(1, st);
+  CQ_CUDA(cudaMemsetAsync(U.tile_counter.p, 0, sizeof(int), st));
+  M.tile_counter = U.tile_counter.p;
   const size_t smem = sizeof(Smem) + 1024;
   CQ_CUDA(cudaFuncSetAttribute(k_mult_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_mult_umma<<<U.n_tiles, kThreads, smem, st>>>(M);
+  int dev_id = 0, sms = 0;
+  CQ_CUDA(cudaGetDevice(&dev_id));
+  CQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id));
+  k_mult_umma<<<std::min(U.n_tiles, 2 * sms), kThreads, smem, st>>>(M, U.n_tiles);
   CQ_CUDA(cudaGetLastError());
   S.launches += 3;
   if (S.prof.on) {

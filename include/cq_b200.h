@@ -274,7 +274,7 @@ int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out)
 #define CQ_OPT_MULT_VARIANT 1
 #define CQ_OPT_BLOCKING_SYNC 2
 /* CQ_OPT_MIXED_KERNEL: kernel of the CQ_PREC_BF16X3 products.  -1 (default) = chosen per product
- * by a fixed rule (the tiles where at least 15 % of their issued tensor work is useful), so a product
+ * by a fixed rule (the tiles where at least 11 % of their issued tensor work is useful), so a product
  * always gives the same bits; 0 = dense 128 x 128 tiles on the tcgen05 tensor cores with TMEM
  * accumulators, operands staged by bulk copies (every block size 4..16; other systems use 1);
  * 1 = one padded 16 x 16 block per warp-level mma.sync. */
