@@ -364,6 +364,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mixed-sample-only", action="store_true",
                     help="run only the mixed-precision vs FP64 comparison on the DZP sample (with --tol, --max-outer)")
+    ap.add_argument("--mixed-handover", type=float, default=None,
+                    help="mixed-sample: residual at which the split-precision phase hands over to FP64 (default 1e-6)")
     ap.add_argument("--no-mixed-sample", action="store_true",
                     help="skip the mixed-precision vs FP64 comparison on the bounded DZP sample")
     ap.add_argument("--workload", default="lnv512", choices=["lnv512", "batch", "serve", "mult216", "mult512", "mult4096"],
@@ -386,6 +388,10 @@ def main():
     ap.add_argument("--nmin", type=int, default=64)
     ap.add_argument("--nmax", type=int, default=1000)
     ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--batch-products", action="store_true",
+                    help="batch / serve: gather the slots' FP64 products into shared persistent launches")
+    ap.add_argument("--fp64-slots", action="store_true",
+                    help="batch / serve: also run the FP64 path on the slots, without and with gathered products")
     ap.add_argument("--rate", type=float, default=200.0)
     ap.add_argument("--tol", type=float, default=None, help="batch/serve: residual tolerance of both arms")
     ap.add_argument("--max-outer", type=int, default=None, help="batch/serve: FindMinDM pass limit per request")
@@ -405,7 +411,7 @@ def main():
         import torch
         import cq_b200
         torch.cuda.set_device(local)
-        emit({"mixed_vs_fp64": mixed_vs_fp64(cq_b200, args.tol, args.max_outer)})
+        emit({"mixed_vs_fp64": mixed_vs_fp64(cq_b200, args.tol, args.max_outer, args.mixed_handover)})
         return
     if args.cpu_full_solve:
         if rank == 0:
@@ -587,18 +593,24 @@ def request_set(n_req, nmin, nmax, seed):
         if k % 2 == 0:
             c, cell = inputs.si_cluster(n, sigma=0.1, seed=1000 + k)
         else:
-            m = int(np.clip(round((n / 8.0) ** (1.0 / 3.0)), 2, 6))
+            m = int(np.clip(round((n / 8.0) ** (1.0 / 3.0)), 2, 10))
             c, cell = inputs.diamond_si(m, sigma=0.1, seed=1000 + k)
-        nsf = 4 if (k // 2) % 2 == 0 else 13
+        # 4x4 and 13x13 blocks alternate in pairs up to 1000 atoms (the batched configuration's range);
+        # larger systems of the served range use 4x4 blocks (a 13x13 system of several thousand atoms
+        # needs some 25 GB per matrix of its 42-bohr range)
+        nsf = 4 if ((k // 2) % 2 == 0 or len(c) > 1000) else 13
         ne = float(len(c)) if nsf == 4 else 2.0 * len(c)
         out.append(dict(coords=c, cell=cell, nsf=nsf, ne=ne, seed=5000 + k, n=len(c)))
     return out
 
 
-def run_server(cq_b200, reqs, n_slots, mixed, rate=None, seed=0):
-    """Submit the requests (all at once, or as a Poisson stream of `rate` per second) and wait for all."""
+def run_server(cq_b200, reqs, n_slots, mixed, rate=None, seed=0, batch_products=False, **lnv):
+    """Submit the requests (all at once, or as a Poisson stream of `rate` per second) and wait for all.
+    batch_products: the slots' FP64 products are gathered into shared persistent launches; lnv: further
+    solver parameters (cq_lnv_params fields)."""
     srv = cq_b200.Server(n_slots=n_slots, hbm_budget=int(0.8 * torch_total_mem()), tolerance=SERVE_TOL,
-                         max_outer=SERVE_MAX_OUTER)
+                         batch_products=batch_products,
+                         max_outer=SERVE_MAX_OUTER, **lnv)
     t_arr = np.zeros(len(reqs))
     if rate:
         t_arr = np.cumsum(np.random.default_rng(seed).exponential(1.0 / rate, size=len(reqs)))
@@ -631,7 +643,7 @@ MIXED_SAMPLE_TOL = 1e-8    # residual at which both arms of the mixed-precision 
 MIXED_SAMPLE_MAX_OUTER = 12
 
 
-def mixed_vs_fp64(cq_b200, tol=None, max_outer=None):
+def mixed_vs_fp64(cq_b200, tol=None, max_outer=None, handover=None):
     """The precision form against the plain FP64 path on the bounded DZP sample: FP64 solves one at a
     time, mixed-precision solves on 4 concurrent slots; both stop at residual `tol` (pass limit
     `max_outer`).  Solves/s of both arms, their ratio, and |dE| per atom of every request."""
@@ -642,7 +654,8 @@ def mixed_vs_fp64(cq_b200, tol=None, max_outer=None):
     try:
         reqs = mixed_sample_requests()
         fp, t_fp = run_server(cq_b200, reqs, 1, False)
-        mx, t_mx = run_server(cq_b200, reqs, 4, True)
+        extra = {} if handover is None else {"mixed_tolerance": float(handover)}
+        mx, t_mx = run_server(cq_b200, reqs, 4, True, **extra)
         tol_used, mo_used = SERVE_TOL, SERVE_MAX_OUTER
     finally:
         SERVE_TOL, SERVE_MAX_OUTER = saved
@@ -655,7 +668,8 @@ def mixed_vs_fp64(cq_b200, tol=None, max_outer=None):
             "fp64": {"solves_per_s": len(reqs) / t_fp, "seconds": t_fp, "slots": 1},
             "mixed": {"solves_per_s": len(reqs) / t_mx, "seconds": t_mx, "slots": 4,
                       "precision": "bf16x3 split products (tensor cores), FP64 traces, line search, Hotelling, "
-                                   "McWeeny start and FP64 continuation from residual 1e-6"},
+                                   "McWeeny start and FP64 continuation from residual %g" %
+                                   (1e-6 if handover is None else handover)},
             "ratio": t_fp / t_mx,
             "max_abs_dE_per_atom_Ha_converged": max(both) if both else None,
             "per_request": per,
@@ -685,7 +699,12 @@ def serve_main(args):
     run_server(cq_b200, warm, 2, True)
     with ClockSampler(0) as clk:
         fp, t_fp = run_server(cq_b200, reqs, 1, False)
-        mx, t_mx = run_server(cq_b200, reqs, args.slots, True, rate=rate, seed=11)
+        mx, t_mx = run_server(cq_b200, reqs, args.slots, True, rate=rate, seed=11, batch_products=args.batch_products)
+        fps = fpb = None
+        if args.fp64_slots:
+            # the FP64 path on the same slots: products launched per solve, then gathered across the slots
+            fps, t_fps = run_server(cq_b200, reqs, args.slots, False, rate=rate, seed=11)
+            fpb, t_fpb = run_server(cq_b200, reqs, args.slots, False, rate=rate, seed=11, batch_products=True)
     bad = [r for r in fp + mx if r["status"] != 0]
     ok = [(a, b) for a, b in zip(fp, mx) if a["status"] == 0 and b["status"] == 0 and a["converged"] and b["converged"]]
     err = max([abs(a["energy"] - b["energy"]) / a["n_atoms"] for a, b in ok], default=None)
@@ -705,6 +724,12 @@ def serve_main(args):
                       "latency_ms_p50": float(np.percentile([r["latency"] * 1e3 for r in fp], 50)),
                       "block_mult_flops": flops_fp64},
         "speedup_vs_fp64_path": t_fp / t_mx,
+        "fp64_on_slots": None if fps is None else {
+            "slots": args.slots, "solves_per_s": len(reqs) / t_fps,
+            "products_gathered_solves_per_s": len(reqs) / t_fpb,
+            "identical_results_gathered": all(a["energy"] == b["energy"] and a["n_products"] == b["n_products"]
+                                              for a, b in zip(fps, fpb) if a["status"] == 0 and b["status"] == 0)},
+        "batch_products": bool(args.batch_products),
         "max_energy_error_per_atom": err,
         "failed": len(bad), "converged": sum(r["converged"] for r in mx),
         "failures": [{"n_atoms": r["n_atoms"], "mixed": r["mixed"], "message": r["message"]} for r in bad][:8],
