@@ -660,6 +660,8 @@ def mixed_vs_fp64(cq_b200, tol=None, max_outer=None, handover=None):
     finally:
         SERVE_TOL, SERVE_MAX_OUTER = saved
     per = [{"n": a["n_atoms"], "fp64_converged": int(a["converged"]), "mixed_converged": int(b["converged"]),
+            "fp64_residual": a["residual"], "mixed_residual": b["residual"],
+            "fp64_electrons": a["electrons"], "mixed_electrons": b["electrons"],
             "dE_per_atom_Ha": (b["energy"] - a["energy"]) / a["n_atoms"], "fp64_s": a["t_done"] - a["t_admit"],
             "mixed_s": b["t_done"] - b["t_admit"]} for a, b in zip(fp, mx) if a["status"] == 0 and b["status"] == 0]
     both = [abs(r["dE_per_atom_Ha"]) for r in per if r["fp64_converged"] and r["mixed_converged"]]

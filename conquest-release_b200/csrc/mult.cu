@@ -14,9 +14,10 @@
 //
 // The bound is the L2/HBM traffic of the operand blocks (an nd x nd FP64 block
 // pair per triple, 2 nd^3 flops): for nd = 4 this is 256 B per 128 flops.  The 4 x 4 kernels write
-// their output blocks with streaming (evict-first) stores: an output range is often larger than L2
-// (the 42-bohr range of the 512-atom cell: 152 MB) and would otherwise push the operand blocks,
-// which every output block re-reads, out of L2.
+// their output blocks with streaming (evict-first) stores, and every kernel reads its pair list (8
+// bytes per triple, each read once) with streaming loads: an output range and a pair list are often
+// larger than L2 (the 42-bohr range of the 512-atom cell: 152 MB; the pair list of LS.L -> LSL: 272 MB)
+// and would otherwise push the operand blocks, which every output block re-reads, out of L2.
 #include <algorithm>
 #include <memory>
 #include <numeric>
@@ -66,7 +67,7 @@ __global__ void __launch_bounds__(256) k_mult_generic(MultArgs M) {
   for (int r = 0; r < 8; ++r) acc[r] = 0.0;
   const int64_t p0 = M.ptr[q], p1 = M.ptr[q + 1];
   for (int64_t t = p0; t < p1; ++t) {
-    int2 pr = M.pairs[t];
+    int2 pr = __ldcs(M.pairs + t);
     const double* X = M.x + M.x_elem[pr.x];
     const double* B = M.b + M.b_elem[pr.y];
     if (TYPE == 1) {
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(256) k_mult_nd4(MultArgs M) {
   double acc = 0.0;
   const int64_t p0 = M.ptr[g], p1 = M.ptr[g + 1];
   for (int64_t t = p0; t < p1; ++t) {
-    int2 pr = M.pairs[t];
+    int2 pr = __ldcs(M.pairs + t);
     const double* X = M.x + M.x_elem[pr.x];
     const double* B = M.b + M.b_elem[pr.y];
     if (TYPE == 1) {
@@ -148,7 +149,7 @@ __global__ void __launch_bounds__(128) k_mult_nd4_tpb(MultArgs M) {
   for (int e = 0; e < 16; ++e) acc[e] = 0.0;
   const int64_t p0 = M.ptr[q], p1 = M.ptr[q + 1];
   for (int64_t t = p0; t < p1; ++t) {
-    int2 pr = M.pairs[t];
+    int2 pr = __ldcs(M.pairs + t);
     const double2* X2 = reinterpret_cast<const double2*>(M.x + 16 * (int64_t)pr.x);
     const double2* B2 = reinterpret_cast<const double2*>(M.b + 16 * (int64_t)pr.y);
     double x[16], b[16];
@@ -210,7 +211,7 @@ __global__ void __launch_bounds__(128) k_mult_nd4_rows(MultArgs M, const int4* _
     for (int v = threadIdx.x; v < (c1 - c0) * 8; v += blockDim.x) xs[v] = __ldg(X2g + (int64_t)c0 * 8 + v);
     __syncthreads();
     while (t < tend) {
-      const int2 pr = M.pairs[t];
+      const int2 pr = __ldcs(M.pairs + t);
       if (pr.x >= c1) break;
       double x[16], b[16];
       const double2* B2 = B2g + (int64_t)pr.y * 8;
@@ -285,11 +286,11 @@ __device__ __forceinline__ void warp_nd4_staged(const MultArgs& M, const int* __
   const double2* Xg = reinterpret_cast<const double2*>(M.x);
   const double2* Bg = reinterpret_cast<const double2*>(M.b);
   const int chunk = lane & 7;
-  int2 pr_next = t < tend ? M.pairs[t] : make_int2(-1, -1);   // pair of the next step, loaded a step ahead
+  int2 pr_next = t < tend ? __ldcs(M.pairs + t) : make_int2(-1, -1);   // pair of the next step, loaded a step ahead
   while (__any_sync(kFull, t < tend)) {
     const bool act = t < tend;
     const int2 pr = pr_next;
-    pr_next = t + 1 < tend ? M.pairs[t + 1] : make_int2(-1, -1);
+    pr_next = t + 1 < tend ? __ldcs(M.pairs + t + 1) : make_int2(-1, -1);
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int src = 4 * j + (lane >> 3);
@@ -376,11 +377,11 @@ __global__ void __launch_bounds__(128, 8) k_mult_nd4_quad(MultArgs M, const int*
   double2* X = sx[warp] + qd * kStride;          // this quad's staged block
   const double2* Xg = reinterpret_cast<const double2*>(M.x);
   const double2* Bg = reinterpret_cast<const double2*>(M.b);
-  int2 pr_next = t < tend ? M.pairs[t] : make_int2(-1, -1);   // pair of the next step, loaded a step ahead
+  int2 pr_next = t < tend ? __ldcs(M.pairs + t) : make_int2(-1, -1);   // pair of the next step, loaded a step ahead
   while (__any_sync(kFull, t < tend)) {
     const bool act = t < tend;                   // uniform over the quad
     const int2 pr = pr_next;
-    pr_next = t + 1 < tend ? M.pairs[t + 1] : make_int2(-1, -1);
+    pr_next = t + 1 < tend ? __ldcs(M.pairs + t + 1) : make_int2(-1, -1);
     double bc[4];
     if (act) {
       X[m] = __ldg(Xg + (int64_t)pr.x * 8 + m);
@@ -446,7 +447,7 @@ __device__ __forceinline__ void warp_tile(const MultArgs& M, int q) {
   const int64_t p0 = M.ptr[q], p1 = M.ptr[q + 1];
   if (live) {
     for (int64_t t = p0; t < p1; ++t) {
-      const int2 pr = M.pairs[t];
+      const int2 pr = __ldcs(M.pairs + t);
       const double* X = M.x + M.x_elem[pr.x];
       const double* B = M.b + M.b_elem[pr.y];
       if (TYPE == 1) {
