@@ -306,6 +306,10 @@ class System:
                                            ctypes.byref(u)))
         return t.value, f.value, bool(u.value)
 
+    def test_stall_next_tensor_product(self):
+        """Test hook (CQ_OPT_TEST_STALL): the next tensor-core product's bounded waits run out."""
+        check(lib().cq_system_set_option(self._h, 4, 1))
+
     def set_mixed_kernel(self, k):
         """Kernel of the split-precision products: -1 = chosen per product by the tile plan's useful fraction
         (default), 0 = tcgen05 tiles, 1 = one block per mma.sync warp."""

@@ -286,6 +286,7 @@ int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, doub
     if (mult_type == 1) CQ_CUDA(cudaMemcpyAsync(c, sys->hc.p, lc * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
     else CQ_CUDA(cudaMemcpyAsync(a, sys->ha.p, la * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
     CQ_CUDA(cudaStreamSynchronize(S.stream));
+    umma_check(S);
   });
 }
 
@@ -354,7 +355,11 @@ int cq_matrix_product_trace(cq_system* sys, int r, const double* a_dev, const do
 }
 
 int cq_synchronize(cq_system* sys) {
-  return guarded([&] { check_sys(sys); CQ_CUDA(cudaStreamSynchronize(sys->S.stream)); });
+  return guarded([&] {
+    check_sys(sys);
+    CQ_CUDA(cudaStreamSynchronize(sys->S.stream));
+    umma_check(sys->S);
+  });
 }
 
 int cq_system_set_stream(cq_system* sys, void* stream) {
@@ -399,6 +404,8 @@ int cq_system_set_option(cq_system* sys, int option, int value) {
       sys->S.mult_variant = value;
     } else if (option == CQ_OPT_BLOCKING_SYNC) {
       sys->S.blocking_sync = value != 0;
+    } else if (option == CQ_OPT_TEST_STALL) {
+      sys->S.umma_test_stall = value != 0;
     } else if (option == CQ_OPT_MIXED_KERNEL) {
       CQ_CHECK(value >= -1 && value <= 1, CQ_ERR_ARG,
                "mixed kernel must be -1 (timed choice), 0 (tcgen05 tiles) or 1 (mma.sync blocks)");

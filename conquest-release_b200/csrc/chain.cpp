@@ -114,16 +114,23 @@ void LNVSolver::solve() {
   // split-precision phase to the hand-over residual, optional FP64 McWeeny purification sweeps,
   // then FP64 FindMinDM from that L to the final tolerance
   const double tol = prm.tolerance;
+  const int max_outer_all = prm.max_outer;
   use_mixed = true;
   prm.tolerance = prm.mixed_tolerance;
+  // the split phase gets at most two passes and leaves at least one to the FP64 continuation: where
+  // the split products' rounding keeps the residual above the hand-over (small dense clusters), a
+  // stalled split phase must not use up the passes the FP64 phase needs
+  prm.max_outer = std::max(1, std::min(max_outer_all - 1, 2));
   try {
     find_min_dm(true);
   } catch (...) {
     prm.tolerance = tol;
+    prm.max_outer = max_outer_all;
     use_mixed = false;
     throw;
   }
   prm.tolerance = tol;
+  prm.max_outer = max_outer_all;
   use_mixed = false;
   if (prm.fp64_mcw_sweeps > 0) purify(prm.fp64_mcw_sweeps);
   if (!prm.fp64_continue) {

@@ -297,6 +297,7 @@ struct System {
   int mixed_kernel = -1;          // split-precision products: 0 = tcgen05 tiles (umma.cu), 1 = mma.sync per block,
                                   // -1 = chosen per product by the tile plan's useful fraction
   int* umma_err_host = nullptr;   // mapped host word set by a tensor-core product whose bounded wait ran out
+  int umma_test_stall = 0;        // test hook (CQ_OPT_TEST_STALL): the next tensor-core product stalls
   int* umma_err_dev = nullptr;
   cudaStream_t stream = nullptr;  // the stream all work of the system is enqueued on
   int uniform_nsf = 0;            // block size when every atom has the same one, else 0

@@ -257,6 +257,7 @@ struct UmmaArgs {
   double* __restrict__ out;
   int* err;                           // mapped host word: a bounded wait ran out
   int* tile_counter;                  // next tile to take (zeroed before the launch)
+  int test_stall;                     // test hook: the copy thread stops after publishing its first tile
 };
 
 // Persistent: the bulk-copy thread of each CTA takes the next tile from a device-wide counter when it
@@ -304,6 +305,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_mult_umma(UmmaArgs P, int n_til
         sm.tile_ring[slot] = t < n_tiles ? t : -1;
         mbar_arrive(&sm.tile_full[slot]);
         if (t >= n_tiles) break;
+        if (P.test_stall) break;       // no stage of the tile will arrive: the MMA thread's wait runs out
         const UmmaTile T = P.tiles[t];
         for (int u0 = 0; u0 < T.n_u; u0 += kUnitsPerStage, ++it) {
           const int s = it % kStages;
@@ -838,6 +840,8 @@ void mat_mult_umma(System& S, int mult_type, int ra, int rb, int rc, double* a, 
   if (!U.tile_counter.n) U.tile_counter.alloc(1, st);
   CQ_CUDA(cudaMemsetAsync(U.tile_counter.p, 0, sizeof(int), st));
   M.tile_counter = U.tile_counter.p;
+  M.test_stall = S.umma_test_stall;
+  S.umma_test_stall = 0;              // one product only
   const size_t smem = sizeof(Smem) + 1024;
   CQ_CUDA(cudaFuncSetAttribute(k_mult_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev_id = 0, sms = 0;

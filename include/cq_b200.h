@@ -279,6 +279,11 @@ int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out)
  * accumulators, operands staged by bulk copies (every block size 4..16; other systems use 1);
  * 1 = one padded 16 x 16 block per warp-level mma.sync. */
 #define CQ_OPT_MIXED_KERNEL 3
+/* CQ_OPT_TEST_STALL (test hook): 1 = in the next tensor-core product the bulk-copy thread stops after
+ * taking its first tile, so the kernel's bounded waits run out (about a second) and the call that
+ * synchronises (cq_mat_mult_host, cq_synchronize, the chain's waits) returns CQ_ERR_TIMEOUT; the
+ * context stays usable and the product's output is not valid.  One product, then back to 0. */
+#define CQ_OPT_TEST_STALL 4
 int cq_system_set_option(cq_system* sys, int option, int value);
 
 /* ------------------------------------------------------------------------ */
@@ -305,8 +310,9 @@ typedef struct {
                               residual stalled above `tolerance` never reaches: the solve then stops with
                               converged = 0 */
   int mixed;               /* 1: cq_lnv_solve runs FindMinDM (McWeeny start included) with CQ_PREC_BF16X3
-                              products to `mixed_tolerance`, then continues from that L with FP64 products
-                              to `tolerance`; Hotelling, traces, line search and Pulay stay FP64 */
+                              products to `mixed_tolerance` (at most two passes, leaving at least one of
+                              `max_outer`), then continues from that L with FP64 products to `tolerance`;
+                              Hotelling, traces, line search and Pulay stay FP64 */
   double mixed_tolerance;  /* residual at which the split-precision phase hands over to FP64 (1e-6) */
   int fp64_mcw_sweeps;     /* FP64 McWeeny purification sweeps of L between the two phases (0) */
   int graphs;              /* 1: each LNV_matrix_multiply call is captured once in a CUDA graph and replayed

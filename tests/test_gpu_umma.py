@@ -125,3 +125,21 @@ def test_repeatable_bits(cfg1):
     got1, _, _ = _run(o, g, 1, 0, 1, 2, bls[0], bls[1], bls[2], 71)
     got2, _, _ = _run(o, g, 1, 0, 1, 2, bls[0], bls[1], bls[2], 71)
     assert np.array_equal(got1, got2)
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(cfg1):
+    """A tensor-core product whose bulk-copy thread stops after taking its first tile (test hook): the
+    MMA thread's bounded wait runs out after about a second, the kernel drains and releases its tensor
+    memory, and the host reports CQ_ERR_TIMEOUT.  The next product on the same context is correct."""
+    import cq_b200
+    o, g, bls = cfg1
+    g.set_mixed_kernel(0)
+    a = inputs.random_blocks(bls[0], 81, inputs.TAG_RANDOM_A)
+    b = inputs.random_blocks(bls[1], 81, inputs.TAG_RANDOM_B)
+    out = np.zeros(bls[2].length)
+    g.test_stall_next_tensor_product()
+    with pytest.raises(cq_b200.CQError) as ei:
+        g.mat_mult_host(1, 0, 1, 2, a, b, out, precision=cq_b200.PREC_BF16X3)
+    assert ei.value.code == cq_b200.CQ_ERR_TIMEOUT
+    got, ref, bound = _run(o, g, 1, 0, 1, 2, bls[0], bls[1], bls[2], 82)
+    _assert_bound(got, ref, bound)
