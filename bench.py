@@ -373,7 +373,7 @@ def main():
                          "many systems on concurrent slots vs the FP64 path one at a time; mult216 / mult512: single "
                          "block products (216-atom DZP C=A.B; the products of one 512-atom LNV call)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3"])
-    ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (-1 autotuned, 0..3, 5)")
+    ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (-1 autotuned, 0..3, 5, 6)")
     ap.add_argument("--mixed-kernel", type=int, default=-1, choices=[-1, 0, 1],
                     help="split-precision products: -1 = chosen per product by the tile plan's useful fraction "
                          "(default), 0 = tcgen05 tiles, 1 = one block per mma.sync warp")

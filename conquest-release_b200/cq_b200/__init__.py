@@ -293,11 +293,11 @@ class System:
         """FP64: (variant chosen by the autotuner or -1, {variant: timed ms}); mixed=True: (output blocks per
         warp chosen for the split-precision kernel or -1, {group size: timed ms})."""
         v, g = c_int(), c_int()
-        ms, gms = (ctypes.c_float * 6)(), (ctypes.c_float * 4)()
+        ms, gms = (ctypes.c_float * 7)(), (ctypes.c_float * 4)()
         check(lib().cq_product_tuning(self._h, mult_type, ra, rb, rc, ctypes.byref(v), ms, ctypes.byref(g), gms))
         if mixed:
             return g.value, {gs: gms[i] for i, gs in enumerate((1, 2, 4, 8)) if gms[i] > 0}
-        return v.value, {i: ms[i] for i in range(6) if ms[i] > 0}
+        return v.value, {i: ms[i] for i in range(7) if ms[i] > 0}
 
     def product_tensor_work(self, mult_type, ra, rb, rc):
         """(tiles, issued tensor flops, usable) of the product's tcgen05 tile plan (cq_product_tensor_work)."""
@@ -340,7 +340,8 @@ class System:
 
     def set_mult_variant(self, v):
         """FP64 4x4 product kernel: -1 = autotuned per product (default), 0 = one lane per output element,
-        1 = one thread per output block, 2 = operand row staged in shared memory, 3 = warp-staged operand blocks."""
+        1 = one thread per output block, 2 = operand row staged in shared memory, 3 = warp-staged operand blocks,
+        5 = four lanes per output block, 6 = operand blocks staged by bulk copies."""
         check(lib().cq_system_set_option(self._h, 1, int(v)))
 
     def profile(self, on=True):

@@ -305,7 +305,7 @@ int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int
     check_sys(sys); check_range(sys, ra); check_range(sys, rb); check_range(sys, rc);
     ProductPlan& P = get_plan(sys->S, mult_type, ra, rb, rc);
     if (variant) *variant = P.tuned;
-    if (ms) for (int v = 0; v < 6; ++v) ms[v] = P.tune_ms[v];
+    if (ms) for (int v = 0; v < 7; ++v) ms[v] = P.tune_ms[v];
     auto it = sys->S.mplans.find(std::make_tuple(mult_type, ra, rb, rc));
     const MixedPlan* M = it == sys->S.mplans.end() ? nullptr : it->second.get();
     static const int kGs[4] = {1, 2, 4, 8};
@@ -400,7 +400,7 @@ int cq_system_set_option(cq_system* sys, int option, int value) {
   return guarded([&] {
     check_sys(sys);
     if (option == CQ_OPT_MULT_VARIANT) {
-      CQ_CHECK(value >= -1 && value <= 5, CQ_ERR_ARG, "mult variant must be -1 (autotuned) or 0..5");
+      CQ_CHECK(value >= -1 && value <= 6, CQ_ERR_ARG, "mult variant must be -1 (autotuned) or 0..6");
       sys->S.mult_variant = value;
     } else if (option == CQ_OPT_BLOCKING_SYNC) {
       sys->S.blocking_sync = value != 0;

@@ -208,7 +208,7 @@ struct ProductPlan {
   DevBuf<int4> tiles;
   DevBuf<int> order;              // output blocks by descending pair count (warp-staged 4x4 kernel)
   int tuned = -1;                 // FP64 kernel variant chosen by the autotuner (-1: not tuned yet)
-  float tune_ms[6] = {0, 0, 0, 0, 0, 0};
+  float tune_ms[7] = {0, 0, 0, 0, 0, 0, 0};
 };
 
 // Split-precision tensor-core product: pair lists sorted by the first operand block,
@@ -313,7 +313,8 @@ struct System {
   int mult_variant = -1;          // 4x4 FP64 product kernel: -1 = chosen per product by the autotuner,
                                   // 0 = one lane per element, 1 = one thread per block,
                                   // 2 = one thread per block with the operand row staged in shared memory,
-                                  // 3 = one thread per block with warp-cooperative staging of the operand blocks;
+                                  // 3 = one thread per block with warp-cooperative staging of the operand blocks,
+                                  // 5 = four lanes per block, 6 = one thread per block with bulk-copy staging;
                                   // other block sizes: 0 = generic warp per block, 4 = warp per block with
                                   // 4 x 2 register tiles per lane
   bool blocking_sync = false;     // host waits sleep on a blocking-sync event instead of spinning
@@ -368,7 +369,8 @@ void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a,
 UmmaPlan& get_umma_plan(System& S, int mult_type, int ra, int rb, int rc);
 bool umma_usable(System& S, int mult_type, int ra, int rb, int rc);
 void mat_mult_umma(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c);
-void umma_check(System& S);       // throws CQ_ERR_TIMEOUT if a tensor-core product's wait ran out
+void umma_check(System& S);       // throws CQ_ERR_TIMEOUT if a kernel's bounded wait ran out
+int* device_timeout_word(System& S);   // mapped host word the bounded waits of the system's kernels set
 size_t umma_smem_bytes();
 
 // algebra.cu

@@ -792,7 +792,7 @@ static void umma_materialise(System& S, UmmaPlan& U) {
   U.materialised = true;
 }
 
-static int* umma_err_word(System& S) {
+int* device_timeout_word(System& S) {
   if (!S.umma_err_host) {
     CQ_CUDA(cudaHostAlloc((void**)&S.umma_err_host, sizeof(int), cudaHostAllocMapped));
     *S.umma_err_host = 0;
@@ -836,7 +836,7 @@ void mat_mult_umma(System& S, int mult_type, int ra, int rb, int rc, double* a, 
   M.xslabs = U.xslabs.p; M.bslabs = U.bslabs.p;
   M.o_elem = O.nb_elem.p;
   M.out = mult_type == 1 ? c : a;
-  M.err = umma_err_word(S);
+  M.err = device_timeout_word(S);
   if (!U.tile_counter.n) U.tile_counter.alloc(1, st);
   CQ_CUDA(cudaMemsetAsync(U.tile_counter.p, 0, sizeof(int), st));
   M.tile_counter = U.tile_counter.p;
@@ -860,7 +860,7 @@ void mat_mult_umma(System& S, int mult_type, int ra, int rb, int rc, double* a, 
 void umma_check(System& S) {
   if (S.umma_err_host && *(volatile int*)S.umma_err_host) {
     *S.umma_err_host = 0;
-    throw Error(CQ_ERR_TIMEOUT, "tensor-core product: a bounded pipeline wait ran out");
+    throw Error(CQ_ERR_TIMEOUT, "block product: a bounded wait of the kernel ran out (bulk copy or pipeline stage never completed)");
   }
 }
 

@@ -173,7 +173,7 @@ int cq_grab_matrix(cq_system* sys, int r, double* a_dev, const char* path, int64
 int cq_product_work(cq_system* sys, int mult_type, int ra, int rb, int rc, int64_t* triples, int64_t* flops);
 
 /* Autotuner record of one product: the FP64 kernel variant it chose (-1 before the product's
- * first autotuned call) and the timed milliseconds of each candidate variant (ms[6], 0 = not
+ * first autotuned call) and the timed milliseconds of each candidate variant (ms[7], 0 = not
  * timed); for its split-precision form the output blocks per warp it chose (1, 2, 4 or 8; -1 =
  * not tuned yet) and the timed milliseconds of those four group sizes (group_ms[4]). */
 int cq_product_tuning(cq_system* sys, int mult_type, int ra, int rb, int rc, int* variant, float* ms, int* group,
@@ -264,9 +264,11 @@ int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out)
  * block, 2 = one thread per output block with the first operand's row staged in shared memory,
  * 3 = one thread per output block with the warp staging the operand blocks through shared
  * memory, 5 = four lanes per output block (one column each), the first operand's block staged
- * in shared memory; for other block sizes (DZP 13 x 13, mixed sizes) 0 = one warp per output
- * block, one lane per element, 4 = one warp per output block, a 4 x 2 register tile per lane (the
- * autotuner candidates are 3/5/1/0 for uniform 4 x 4 blocks and 4/0 otherwise).  All give
+ * in shared memory, 6 = one thread per output block with its operand blocks staged by bulk copies
+ * (cp.async.bulk, completion on an mbarrier, bounded waits); for other block sizes (DZP 13 x 13,
+ * mixed sizes) 0 = one warp per output block, one lane per element, 4 = one warp per output block,
+ * a 4 x 2 register tile per lane (the autotuner candidates are 3/5/1/0 for uniform 4 x 4 blocks
+ * and 4/0 otherwise; variant 6 is selectable only).  All give
  * identical results.
  * CQ_OPT_BLOCKING_SYNC: 1 = the host thread sleeps on a blocking-sync event whenever the
  * solver waits for a scalar from the device (many concurrent solvers per host core), 0 = it

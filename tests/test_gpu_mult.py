@@ -138,7 +138,7 @@ LNV_PRODUCTS = [  # (type, a range, b range, c range) in mat_mult roles, from th
 ]
 
 
-@pytest.mark.parametrize("variant", [-1, 0, 1, 2, 3, 5])
+@pytest.mark.parametrize("variant", [-1, 0, 1, 2, 3, 5, 6])
 @pytest.mark.parametrize("prod", LNV_PRODUCTS)
 def test_lnv_products_sz_bit_exact(cfg2, prod, variant):
     o, g, bls, idx = cfg2
