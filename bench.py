@@ -368,11 +368,13 @@ def main():
                     help="mixed-sample: residual at which the split-precision phase hands over to FP64 (default 1e-6)")
     ap.add_argument("--no-mixed-sample", action="store_true",
                     help="skip the mixed-precision vs FP64 comparison on the bounded DZP sample")
-    ap.add_argument("--workload", default="lnv512", choices=["lnv512", "batch", "serve", "mult216", "mult512", "mult4096"],
+    ap.add_argument("--workload", default="lnv512",
+                    choices=["lnv512", "batch", "serve", "mult216", "mult512", "mult216dzp", "mult4096"],
                     help="lnv512: the plain FP64 512-atom solve (default); batch / serve: mixed-precision solves of "
-                         "many systems on concurrent slots vs the FP64 path one at a time; mult216 / mult512: single "
-                         "block products (216-atom DZP C=A.B; the products of one 512-atom LNV call)")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3"])
+                         "many systems on concurrent slots vs the FP64 path one at a time; mult216 / mult512 / "
+                         "mult216dzp / mult4096: single block products (216-atom DZP C=A.B; the products of one LNV "
+                         "call on the 512-atom SZ, 216-atom DZP and 4096-atom DZP cells)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3", "bf16x6"])
     ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (-1 autotuned, 0..3, 5, 6)")
     ap.add_argument("--mixed-kernel", type=int, default=-1, choices=[-1, 0, 1],
                     help="split-precision products: -1 = chosen per product by the tile plan's useful fraction "
@@ -397,7 +399,7 @@ def main():
     ap.add_argument("--max-outer", type=int, default=None, help="batch/serve: FindMinDM pass limit per request")
     args = ap.parse_args()
     ws, rank, local = dist_env()
-    if args.workload in ("mult216", "mult512", "mult4096") and args.impl == "ours":
+    if args.workload in ("mult216", "mult512", "mult216dzp", "mult4096") and args.impl == "ours":
         if rank == 0:
             mult_main(args)
         return
@@ -669,9 +671,9 @@ def mixed_vs_fp64(cq_b200, tol=None, max_outer=None, handover=None):
                       "residual %g (pass limit %d)" % (tol_used, mo_used),
             "fp64": {"solves_per_s": len(reqs) / t_fp, "seconds": t_fp, "slots": 1},
             "mixed": {"solves_per_s": len(reqs) / t_mx, "seconds": t_mx, "slots": 4,
-                      "precision": "bf16x3 split products (tensor cores), FP64 traces, line search, Hotelling, "
-                                   "McWeeny start and FP64 continuation from residual %g" %
-                                   (1e-6 if handover is None else handover)},
+                      "precision": "bf16x6 split products (three bf16 parts, tensor cores, FP64 sums over block "
+                                   "pairs), FP64 traces, line search, Hotelling, McWeeny start and FP64 continuation "
+                                   "from residual %g" % (max(tol_used, 1e-8) if handover is None else handover)},
             "ratio": t_fp / t_mx,
             "max_abs_dE_per_atom_Ha_converged": max(both) if both else None,
             "per_request": per,
@@ -716,7 +718,7 @@ def serve_main(args):
     line = {
         "metric": "LNV solves/s (%s, mixed precision, %d slots)" % ("served" if rate else "batched", args.slots),
         "value": len(reqs) / t_mx, "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
-        "dtype": "bf16x3+f64", "data": "synthetic (seeded Si clusters and supercells, S/H generators)",
+        "dtype": "bf16x6+f64", "data": "synthetic (seeded Si clusters and supercells, S/H generators)",
         "config": {"workload": "lnv_%s_si_mixed" % args.workload, "requests": len(reqs),
                    "atoms": [args.nmin, args.nmax], "atoms_total": atoms, "blocks": "4x4 and 13x13",
                    "ranges_bohr": dict(zip("SHLT", SERVE_RANGES)), "arrival_rate_per_s": rate,
@@ -737,7 +739,9 @@ def serve_main(args):
         "failures": [{"n_atoms": r["n_atoms"], "mixed": r["mixed"], "message": r["message"]} for r in bad][:8],
         "per_request": [{"n": a["n_atoms"], "nsf": q["nsf"], "fp64_s": a["t_done"] - a["t_admit"],
                          "mixed_s": b["t_done"] - b["t_admit"], "conv": [a["converged"], b["converged"]],
-                         "dE_per_atom": (b["energy"] - a["energy"]) / a["n_atoms"]}
+                         "dE_per_atom": (b["energy"] - a["energy"]) / a["n_atoms"],
+                         "products": [a["n_products"], b["n_products"]],
+                         "flops": [a["flops"], b["flops"]], "flops_split_mixed": b["flops_mixed"]}
                         for a, b, q in zip(fp, mx, reqs)],
         "bytes_peak_max": max(r["bytes_peak"] for r in mx),
         "clocks": clk.summary(),
@@ -753,7 +757,9 @@ def mult_main(args):
 
     mult216: C = A.B on a 216-atom Si supercell (3x3x3 cells, sigma 0.05), 13x13 blocks, A range 8,
              B range 12, C range 20, entries uniform[-1,1] exp(-r/3).
-    lnv512:  the nine products of one LNV_matrix_multiply(M3, phi, E) call on the 512-atom SZ workload.
+    mult512 / mult216dzp / mult4096: the nine products of one LNV_matrix_multiply(M3, phi, E) call on the
+             512-atom SZ workload, on a 216-atom DZP cell (3x3x3 cells, sigma 0.1, seed 77) and on the
+             4096-atom DZP cell (8x8x8 cells).
     """
     import torch
     import cq_b200
@@ -763,7 +769,8 @@ def mult_main(args):
     stream = torch.cuda.Stream(device=dev)      # the library's stream, where the events are recorded
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    prec = {"fp64": cq_b200.PREC_FP64, "fma": cq_b200.PREC_FP64_FMA, "bf16x3": cq_b200.PREC_BF16X3}[args.precision]
+    prec = {"fp64": cq_b200.PREC_FP64, "fma": cq_b200.PREC_FP64_FMA, "bf16x3": cq_b200.PREC_BF16X3,
+            "bf16x6": cq_b200.PREC_BF16X6}[args.precision]
     if args.workload == "mult216":
         coords, cell = inputs.diamond_si(3, sigma=0.05, seed=1)
         n = len(coords)
@@ -775,8 +782,8 @@ def mult_main(args):
         desc = "216-atom Si DZP (13x13), A 8 / B 12 / C 20 bohr"
     else:
         from cq_b200 import inputs as _inp
-        ncell, nsf = (4, 4) if args.workload == "mult512" else (8, 13)
-        coords, cell = _inp.diamond_si(ncell, sigma=0.1, seed=2)
+        ncell, nsf = {"mult512": (4, 4), "mult216dzp": (3, 13)}.get(args.workload, (8, 13))
+        coords, cell = _inp.diamond_si(ncell, sigma=0.1, seed=77 if args.workload == "mult216dzp" else 2)
         n = len(coords)
         rng = cq_b200.lnv_ranges(CFG["rs"], CFG["rh"], CFG["rl"], CFG["rt"])
         ridx = {k: i for i, k in enumerate(rng)}
@@ -813,7 +820,7 @@ def mult_main(args):
                 ms.append(e0.elapsed_time(e1))
             m = float(np.median(ms))
             nbytes = 8.0 * (g.length(ra) + g.length(rb) + g.length(rc))
-            tv, tms = g.product_tuning(t, ra, rb, rc, mixed=(args.precision == "bf16x3"))
+            tv, tms = g.product_tuning(t, ra, rb, rc, mixed=(args.precision in ("bf16x3", "bf16x6")))
             tensor = None
             if args.precision == "bf16x3" and args.mixed_kernel != 1:
                 nt, issued, usable = g.product_tensor_work(t, ra, rb, rc)
@@ -826,7 +833,7 @@ def mult_main(args):
     tot_ms = sum(o["ms"] for o in out)
     emit({"metric": "block-mult TFLOP/s (%s)" % args.precision, "value": tot_fl / (tot_ms / 1e3) / 1e12,
           "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-          "dtype": {"fp64": "f64", "fma": "f64", "bf16x3": "bf16x3"}[args.precision],
+          "dtype": {"fp64": "f64", "fma": "f64", "bf16x3": "bf16x3", "bf16x6": "bf16x6"}[args.precision],
           "data": "synthetic", "config": {"workload": args.workload, "system": desc, "variant": args.variant,
                                           "mixed_kernel": args.mixed_kernel,
                                           "l2": "flushed (256 MB write) before every timed launch"},

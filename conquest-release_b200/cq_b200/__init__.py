@@ -27,7 +27,7 @@ P = ctypes.POINTER
 # cq_h_rebuild_fn: (user, K_dev, H_dev, length, stream) -> status
 H_REBUILD_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_void_p, c_void_p, c_int64, c_void_p)
 # product arithmetic (cq_mat_mult precision)
-PREC_FP64_FMA, PREC_FP64, PREC_BF16X3 = 0, 1, 2
+PREC_FP64_FMA, PREC_FP64, PREC_BF16X3, PREC_BF16X6 = 0, 1, 2, 3
 
 
 class LNVParams(ctypes.Structure):
@@ -36,7 +36,8 @@ class LNVParams(ctypes.Structure):
                 ("maxpulaystep", c_double), ("lintol", c_double), ("global_tolerance", c_int), ("vary_mu", c_int),
                 ("invs_max_steps", c_int), ("invs_delta_tol", c_double), ("invs_tol", c_double), ("exact", c_int),
                 ("max_outer", c_int), ("mixed", c_int), ("mixed_tolerance", c_double), ("fp64_mcw_sweeps", c_int),
-                ("graphs", c_int), ("mixed_mcw", c_int), ("fp64_continue", c_int)]
+                ("graphs", c_int), ("mixed_mcw", c_int), ("fp64_continue", c_int), ("split_parts", c_int),
+                ("mixed_max_outer", c_int)]
 
 
 class LNVResult(ctypes.Structure):
@@ -131,6 +132,7 @@ def lib():
         "cq_lnv_put": [c_void_p, ctypes.c_char_p, c_void_p, c_int],
         "cq_lnv_solve_host": [c_void_p, P(c_double), P(c_double), P(c_double), P(c_double), P(LNVResult)],
         "cq_lnv_reduction_log": [c_void_p, c_int, P(c_double), c_int64, P(c_int64)],
+        "cq_lnv_residual_history": [c_void_p, P(c_double), c_int64, P(c_int64)],
         "cq_lnv_force_matrices": [c_void_p, c_void_p, c_void_p, c_int],
     }
     for name, args in lnv_sigs.items():
@@ -232,7 +234,7 @@ class System:
 
     # ---- products and algebra on device memory ------------------------------
     def mat_mult(self, mult_type, ra, rb, rc, a, b, c, exact=True, precision=None):
-        """precision: PREC_FP64 (default kernel rounding), PREC_FP64_FMA, PREC_BF16X3 (tensor cores)."""
+        """precision: PREC_FP64 (default kernel rounding), PREC_FP64_FMA, PREC_BF16X3 or PREC_BF16X6 (tensor cores, two- or three-part split)."""
         prec = int(bool(exact)) if precision is None else int(precision)
         check(lib().cq_mat_mult(self._h, mult_type, ra, rb, rc, _ptr(a), _ptr(b), _ptr(c), prec))
 
@@ -309,6 +311,11 @@ class System:
     def test_stall_next_tensor_product(self):
         """Test hook (CQ_OPT_TEST_STALL): the next tensor-core product's bounded waits run out."""
         check(lib().cq_system_set_option(self._h, 4, 1))
+
+    def set_split_group(self, g):
+        """Output blocks per warp of the mma.sync split-precision kernels: -1 = autotuned (default), 1, 2, 4
+        or 8 (two-part split only); the same bits for every choice."""
+        check(lib().cq_system_set_option(self._h, 5, int(g)))
 
     def set_mixed_kernel(self, k):
         """Kernel of the split-precision products: -1 = chosen per product by the tile plan's useful fraction
@@ -433,9 +440,17 @@ def mat_mult_batch(products):
 def lnv_params(**kw):
     p = LNVParams()
     check(lib().cq_lnv_params_default(ctypes.byref(p)))
-    for k, v in kw.items():
-        setattr(p, k, v)
+    set_params(p, kw)
     return p
+
+
+def set_params(p, kw):
+    """Set cq_lnv_params fields by name; an unknown name is an error (ctypes would take it silently)."""
+    names = {f for f, _ in LNVParams._fields_}
+    for k, v in kw.items():
+        if k not in names:
+            raise TypeError("unknown cq_lnv_params field %r" % k)
+        setattr(p, k, v)
 
 
 class LNV:
@@ -507,6 +522,16 @@ class LNV:
         n = c_int64()
         check(lib().cq_lnv_reduction_log(self._h, int(bool(enable)), _dp(out), cap, ctypes.byref(n)))
         return out[:min(n.value, cap)]
+
+    def residual_history(self):
+        """Per earlyDM / lateDM iteration of the last solve: (residual, band energy, products so far,
+        1.0 if split-precision, seconds since the solve started) rows of an (n, 5) array."""
+        n = c_int64()
+        check(lib().cq_lnv_residual_history(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 5))
+        if n.value:
+            check(lib().cq_lnv_residual_history(self._h, _dp(out), n.value, ctypes.byref(n)))
+        return out
 
     def set_h_rebuild(self, fn):
         """Mixed-L self-consistency (minE.MixedLSelfConsistent): lateDM calls fn(K_ptr, H_ptr, length,
@@ -644,8 +669,7 @@ class Server:
         c.n_slots, c.hbm_budget, c.max_bypass = int(n_slots), int(hbm_budget), int(max_bypass)
         c.blocking_sync, c.dry_run, c.dry_run_seconds = int(bool(blocking_sync)), int(bool(dry_run)), float(dry_run_seconds)
         c.batch_products, c.batch_window_us = int(bool(batch_products)), float(batch_window_us)
-        for k, v in lnv.items():
-            setattr(c.lnv, k, v)
+        set_params(c.lnv, lnv)
         h = c_void_p()
         check(L.cq_server_create(ctypes.byref(c), ctypes.byref(h)))
         self._h = h

@@ -64,11 +64,13 @@ int cq_lnv_params_default(cq_lnv_params* p) {
   p->exact = 1;
   p->max_outer = 40;
   p->mixed = 0;
-  p->mixed_tolerance = 1.0e-6;
+  p->mixed_tolerance = 0.0;
   p->fp64_mcw_sweeps = 0;
   p->graphs = 1;
   p->mixed_mcw = 0;
   p->fp64_continue = 1;
+  p->split_parts = 3;
+  p->mixed_max_outer = 0;
   return CQ_OK;
 }
 
@@ -80,6 +82,8 @@ int cq_lnv_create(cq_system* sys, const int* ranges, double ne_spin, const cq_ln
     if (p) prm = *p;
     CQ_CHECK(prm.maxpulay >= 1 && prm.maxpulay <= 16, CQ_ERR_ARG, "maxpulay must be 1..16");
     CQ_CHECK(ne_spin > 0, CQ_ERR_ARG, "ne_spin must be positive");
+    CQ_CHECK(prm.split_parts == 2 || prm.split_parts == 3, CQ_ERR_ARG, "split_parts must be 2 or 3");
+    CQ_CHECK(prm.mixed_max_outer >= 0, CQ_ERR_ARG, "mixed_max_outer must be >= 0");
     auto s = std::make_unique<cq_lnv>();
     s->solver = std::make_unique<LNVSolver>(system_of(sys), ranges, ne_spin, prm);
     *out = s.release();
@@ -207,6 +211,16 @@ int cq_lnv_reduction_log(cq_lnv* s, int enable, double* out, int64_t cap, int64_
     if (out) std::memcpy(out, L.rlog.data(), sizeof(double) * std::min<int64_t>(cap, (int64_t)L.rlog.size()));
     L.rlog_on = enable != 0;
     L.rlog.clear();
+  });
+}
+
+int cq_lnv_residual_history(cq_lnv* s, double* out, int64_t cap, int64_t* n) {
+  return guarded_call([&] {
+    CQ_CHECK(s && s->solver && n, CQ_ERR_ARG, "null argument");
+    const std::vector<double>& g = s->solver->glog;
+    const int f = LNVSolver::kLogFields;
+    *n = (int64_t)g.size() / f;
+    if (out) std::memcpy(out, g.data(), sizeof(double) * f * std::min<int64_t>(cap, *n));
   });
 }
 

@@ -88,7 +88,7 @@ void LNVSolver::mult_dispatch(ProductPlan& P, double* a, const double* b, double
   if (use_mixed && S.max_nsf > 8) {
     stats.n_products_mixed++;
     stats.flops_mixed += P.flops;
-    mat_mult_mixed(S, P.mult_type, P.ra, P.rb, P.rc, a, b, c);
+    mat_mult_mixed(S, P.mult_type, P.ra, P.rb, P.rc, a, b, c, prm.split_parts);
   } else if (S.batch_submit) {
     S.batch_submit(P, a, b, c, prm.exact);
   } else {
@@ -98,6 +98,8 @@ void LNVSolver::mult_dispatch(ProductPlan& P, double* a, const double* b, double
 
 void LNVSolver::solve() {
   stats = LNVStats();
+  glog.clear();
+  t_solve = std::chrono::steady_clock::now();
   delta_e = 0.0;
   // every solve starts from the state of a new solver: the matrices the chain carries from one
   // call to the next (L, phi, K, T and the products of L) are cleared
@@ -116,11 +118,16 @@ void LNVSolver::solve() {
   const double tol = prm.tolerance;
   const int max_outer_all = prm.max_outer;
   use_mixed = true;
-  prm.tolerance = prm.mixed_tolerance;
-  // the split phase gets at most two passes and leaves at least one to the FP64 continuation: where
-  // the split products' rounding keeps the residual above the hand-over (small dense clusters), a
-  // stalled split phase must not use up the passes the FP64 phase needs
-  prm.max_outer = std::max(1, std::min(max_outer_all - 1, 2));
+  // hand-over residual: the three-part split carries the solve to the final tolerance (its products'
+  // rounding, about 1e-7 of sum |a||b|, stalls the residual near 1e-8 on DZP Si), the two-part split
+  // to 1e-6
+  prm.tolerance = prm.mixed_tolerance > 0 ? prm.mixed_tolerance
+                                          : (prm.split_parts == 3 ? std::max(tol, 1e-8) : 1e-6);
+  // the split phase gets a bounded number of passes and leaves at least one to the FP64 continuation:
+  // where the split products' rounding keeps the residual above the hand-over (small dense clusters
+  // with the two-part split), a stalled split phase must not use up the passes the FP64 phase needs
+  const int split_passes = prm.mixed_max_outer > 0 ? prm.mixed_max_outer : (prm.split_parts == 3 ? 4 : 2);
+  prm.max_outer = std::max(1, std::min(max_outer_all - 1, split_passes));
   try {
     find_min_dm(true);
   } catch (...) {
@@ -724,6 +731,7 @@ int LNVSolver::early_dm(int ndone, bool& inflex) {
     stats.early_iters++;
     stats.last_energy = energy0;
     stats.last_residual = g0;
+    log_iteration(g0, energy0);
     if (std::fabs(zeta) < prm.lintol) return n_iter;
   }
   return ndone;
@@ -828,6 +836,7 @@ int LNVSolver::late_dm(int ndone, bool& done, double& deltaE) {
     stats.late_iters++;
     stats.last_energy = energy1;
     stats.last_residual = g1;
+    log_iteration(g1, energy1);
     if (g1 < prm.tolerance) { done = true; return n_iter; }
     else if (!h_rebuild && g1 > 2.0 * g0) return n_iter;   // no residual-rise exit with the H coupling
     else if (g1 > 0.99 * g0) {

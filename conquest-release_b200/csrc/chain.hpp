@@ -1,5 +1,6 @@
 // LNV / McWeeny solver state (see chain.cpp).
 #pragma once
+#include <chrono>
 #include <initializer_list>
 #include <utility>
 #include <vector>
@@ -64,6 +65,18 @@ class LNVSolver {
   LNVStats stats;
   std::vector<double> rlog;   // every trace / product-trace value in call order, when rlog_on
   bool rlog_on = false;
+  // per earlyDM / lateDM iteration: residual, band energy, products run so far, 1 if the iteration's
+  // products were split-precision, host seconds since the solve started (the residual has just been
+  // read from the device, so the time includes the iteration's device work) -- the reference's
+  // PulayR / PulayE record, DMMinModule.f90:289-294
+  static constexpr int kLogFields = 5;
+  std::vector<double> glog;
+  std::chrono::steady_clock::time_point t_solve = std::chrono::steady_clock::now();
+  void log_iteration(double g, double energy) {
+    if (glog.size() < (size_t)kLogFields << 16)
+      glog.insert(glog.end(), {g, energy, (double)stats.n_products, use_mixed ? 1.0 : 0.0,
+                               std::chrono::duration<double>(std::chrono::steady_clock::now() - t_solve).count()});
+  }
   DMat Smat, Hmat, L, T, Ttran, LS, SL, K, phi;
 
   DMat temp(int rng);

@@ -219,6 +219,8 @@ struct MixedPlan {
   int tuned_g = -1;                 // group size chosen by the autotuner (index into 1, 2, 4, 8)
   int kernel = -1;                  // 0 = tcgen05 tiles, 1 = per-block mma.sync (-1: not chosen yet)
   float tune_ms[4] = {0, 0, 0, 0};
+  int tuned_g6 = -1;                // three-part split: group size chosen (index into 1, 2, 4)
+  float tune_ms6[3] = {0, 0, 0};
   int64_t n_pairs = 0, flops = 0;
   DevBuf<int64_t> own_ptr;        // type 2 only (type 1 uses the FP64 plan's lists, already sorted)
   DevBuf<int2> own_pairs;
@@ -227,7 +229,7 @@ struct MixedPlan {
   DevBuf<int2> groups[4];
 };
 
-struct FragBuf { DevBuf<uint4> hi, lo; };
+struct FragBuf { DevBuf<uint4> hi, lo, mid; };   // mid: three-part split only
 
 // Dense tensor-core tile of a split-precision product (umma.cu): up to 128 output rows (a run of
 // primary atoms) x one column chunk (a run of up to 128 orbitals of cover atoms), contracted over the
@@ -297,6 +299,7 @@ struct System {
   int mixed_kernel = -1;          // split-precision products: 0 = tcgen05 tiles (umma.cu), 1 = mma.sync per block,
                                   // -1 = chosen per product by the tile plan's useful fraction
   int* umma_err_host = nullptr;   // mapped host word set by a tensor-core product whose bounded wait ran out
+  int split_group = -1;           // CQ_OPT_SPLIT_GROUP: forced output blocks per mma.sync split warp (-1 tuned)
   int umma_test_stall = 0;        // test hook (CQ_OPT_TEST_STALL): the next tensor-core product stalls
   int* umma_err_dev = nullptr;
   cudaStream_t stream = nullptr;  // the stream all work of the system is enqueued on
@@ -358,12 +361,14 @@ void ensure_product_order(System& S, ProductPlan& P);   // the 4 x 4 kernels' ou
 void generate_SH(System& S, int r, int which, uint64_t seed, double* out);
 
 // mixed.cu
-void to_fragments(System& S, int r, const double* src, int role_b, int trans, uint4* hi, uint4* lo);
+void to_fragments(System& S, int r, const double* src, int role_b, int trans, uint4* hi, uint4* lo, uint4* mid);
 void launch_mult_tc(System& S, MixedPlan& MP, const uint4* xa_hi, const uint4* xa_lo, const uint4* bb_hi,
                     const uint4* bb_lo, double* out);
 // split-precision mat_mult with the roles of launch_mat_mult: tcgen05 tiles where every block size is
 // 4..128 (unless the system selects the per-block kernel), else the per-block mma.sync kernel
-void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c);
+// parts = 2: BF16x3 (tcgen05 tiles or mma.sync blocks by the fill rule); parts = 3: BF16x6 (mma.sync)
+void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c,
+                    int parts = 2);
 
 // umma.cu
 UmmaPlan& get_umma_plan(System& S, int mult_type, int ra, int rb, int rc);

@@ -3,7 +3,8 @@
 // Each FP64 operand block is padded to 16 x 16 and split into two bf16 parts,
 // v = hi + lo (hi = bf16(v), lo = bf16(v - hi)); a block product is the sum of
 // hi.hi + hi.lo + lo.hi (three bf16 MMAs, FP32 accumulation), which carries
-// about 16 significant bits per term.  The result is written back as FP64 into
+// about 16 significant bits per term.  The three-part split (v = hi + mid + lo,
+// six MMAs per term, FP64 accumulation across terms) carries about 22.  The result is written back as FP64 into
 // the block storage of the output range, so the matrices of the chain stay FP64.
 //
 // Work decomposition (output stationary, same pair lists as the FP64 path):
@@ -41,6 +42,15 @@ __device__ __forceinline__ void split2(double v, __nv_bfloat16& h, __nv_bfloat16
   l = __double2bfloat16(v - (double)__bfloat162float(h));
 }
 
+// v = hi + mid + lo + r with |r| <= 2^-24 |v| (about 2^-25 for round-to-nearest parts): both
+// differences are exact in FP64
+__device__ __forceinline__ void split3(double v, __nv_bfloat16& h, __nv_bfloat16& m, __nv_bfloat16& l) {
+  h = __double2bfloat16(v);
+  const double r1 = v - (double)__bfloat162float(h);
+  m = __double2bfloat16(r1);
+  l = __double2bfloat16(r1 - (double)__bfloat162float(m));
+}
+
 // A-role fragments (M = block rows, K = block columns):
 //   reg0 (row g,   k 2t..2t+1), reg1 (row g+8, k 2t..2t+1), reg2 (row g, k 2t+8..), reg3 (row g+8, k 2t+8..)
 // B-role fragments (K = block rows, N = block columns; `trans` uses the transposed block),
@@ -48,7 +58,7 @@ __device__ __forceinline__ void split2(double v, __nv_bfloat16& h, __nv_bfloat16
 __global__ void k_to_frag(int nnz, const int64_t* __restrict__ elem, const int* __restrict__ row,
                           const int* __restrict__ cover, const int* __restrict__ prim_nsf,
                           const int* __restrict__ cover_nsf, const double* __restrict__ src, int role_b, int trans,
-                          uint4* __restrict__ hi, uint4* __restrict__ lo) {
+                          uint4* __restrict__ hi, uint4* __restrict__ lo, uint4* __restrict__ mid) {
   int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int e = (int)(tid >> 5), lane = (int)(tid & 31);
   if (e >= nnz) return;
@@ -70,16 +80,24 @@ __global__ void k_to_frag(int nnz, const int64_t* __restrict__ elem, const int* 
       }
     }
   }
-  uint32_t wh[4], wl[4];
+  uint32_t wh[4], wm[4], wl[4];
   for (int q = 0; q < 4; ++q) {
-    __nv_bfloat16 h0, l0, h1, l1;
-    split2(blk_at(B, ndr, ndc, rr[2 * q], cc[2 * q]), h0, l0);
-    split2(blk_at(B, ndr, ndc, rr[2 * q + 1], cc[2 * q + 1]), h1, l1);
+    __nv_bfloat16 h0, m0, l0, h1, m1, l1;
+    const double v0 = blk_at(B, ndr, ndc, rr[2 * q], cc[2 * q]), v1 = blk_at(B, ndr, ndc, rr[2 * q + 1], cc[2 * q + 1]);
+    if (mid) {
+      split3(v0, h0, m0, l0);
+      split3(v1, h1, m1, l1);
+      wm[q] = pack_bf16(m0, m1);
+    } else {
+      split2(v0, h0, l0);
+      split2(v1, h1, l1);
+    }
     wh[q] = pack_bf16(h0, h1);
     wl[q] = pack_bf16(l0, l1);
   }
   hi[(int64_t)e * 32 + lane] = make_uint4(wh[0], wh[1], wh[2], wh[3]);
   lo[(int64_t)e * 32 + lane] = make_uint4(wl[0], wl[1], wl[2], wl[3]);
+  if (mid) mid[(int64_t)e * 32 + lane] = make_uint4(wm[0], wm[1], wm[2], wm[3]);
 }
 
 __device__ __forceinline__ void mma_bf16(float (&c)[4], const uint4& a, uint32_t b0, uint32_t b1) {
@@ -98,6 +116,8 @@ struct TCArgs {
   const uint4* __restrict__ xa_lo;
   const uint4* __restrict__ bb_hi;     // B operand, B-role fragments
   const uint4* __restrict__ bb_lo;
+  const uint4* __restrict__ xa_mid;    // middle parts (three-part split only)
+  const uint4* __restrict__ bb_mid;
   const int* __restrict__ o_row;
   const int* __restrict__ o_cover;
   const int64_t* __restrict__ o_elem;
@@ -217,24 +237,180 @@ __global__ void __launch_bounds__(128) k_mult_tc1(TCArgs M) {
     }
 }
 
+// Three-part split (BF16x6): v = hi + mid + lo, one output block per warp.  Per term and n8 half the
+// six products that carry terms down to 2^-16 of hi.hi run into a zeroed FP32 accumulator, smallest
+// first (hi.lo, lo.hi, mid.mid, hi.mid, mid.hi, hi.hi), and the term's 16 x 8 result is added to FP64
+// accumulators, so the FP32 rounding spans one 16-wide contraction rather than the whole sum.  The
+// omitted products (mid.lo, lo.mid, lo.lo) and the split remainders are below 2^-23 of |a||b| per
+// element product.  The next term's six fragments load while the current term's MMAs run.
+__global__ void __launch_bounds__(128) k_mult_tc6(TCArgs M) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= M.n_groups) return;
+  const int q = M.groups[w].x;
+  int64_t p = M.ptr[q];
+  const int64_t pe = M.ptr[q + 1];
+  double acc[2][4];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) acc[h][r] = 0.0;
+  uint4 ah = {0, 0, 0, 0}, am = ah, al = ah, bh = ah, bm = ah, bl = ah;
+  if (p < pe) {
+    const int2 pr = M.pairs[p];
+    ah = __ldg(M.xa_hi + (int64_t)pr.x * 32 + lane);
+    am = __ldg(M.xa_mid + (int64_t)pr.x * 32 + lane);
+    al = __ldg(M.xa_lo + (int64_t)pr.x * 32 + lane);
+    bh = __ldg(M.bb_hi + (int64_t)pr.y * 32 + lane);
+    bm = __ldg(M.bb_mid + (int64_t)pr.y * 32 + lane);
+    bl = __ldg(M.bb_lo + (int64_t)pr.y * 32 + lane);
+  }
+  for (; p < pe; ++p) {
+    uint4 nah = ah, nam = am, nal = al, nbh = bh, nbm = bm, nbl = bl;
+    if (p + 1 < pe) {
+      const int2 pn = M.pairs[p + 1];
+      nah = __ldg(M.xa_hi + (int64_t)pn.x * 32 + lane);
+      nam = __ldg(M.xa_mid + (int64_t)pn.x * 32 + lane);
+      nal = __ldg(M.xa_lo + (int64_t)pn.x * 32 + lane);
+      nbh = __ldg(M.bb_hi + (int64_t)pn.y * 32 + lane);
+      nbm = __ldg(M.bb_mid + (int64_t)pn.y * 32 + lane);
+      nbl = __ldg(M.bb_lo + (int64_t)pn.y * 32 + lane);
+    }
+    float t[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) t[h][r] = 0.f;
+    mma_bf16(t[0], ah, bl.x, bl.y);
+    mma_bf16(t[0], al, bh.x, bh.y);
+    mma_bf16(t[0], am, bm.x, bm.y);
+    mma_bf16(t[0], ah, bm.x, bm.y);
+    mma_bf16(t[0], am, bh.x, bh.y);
+    mma_bf16(t[0], ah, bh.x, bh.y);
+    mma_bf16(t[1], ah, bl.z, bl.w);
+    mma_bf16(t[1], al, bh.z, bh.w);
+    mma_bf16(t[1], am, bm.z, bm.w);
+    mma_bf16(t[1], ah, bm.z, bm.w);
+    mma_bf16(t[1], am, bh.z, bh.w);
+    mma_bf16(t[1], ah, bh.z, bh.w);
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[h][r] += (double)t[h][r];
+    ah = nah; am = nam; al = nal; bh = nbh; bm = nbm; bl = nbl;
+  }
+  const int g = lane >> 2, t4 = lane & 3;
+  const int ndr = M.prim_nsf[M.o_row[q]], ndc = M.cover_nsf[M.o_cover[q]];
+  double* O = M.out + M.o_elem[q];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      int row = g + ((r & 2) ? 8 : 0), col = 8 * h + 2 * t4 + (r & 1);
+      if (row < ndr && col < ndc) O[row + ndr * col] = acc[h][r];
+    }
+}
+
+// Three-part split, G output blocks of one row per warp (G = 2 or 4): each first-operand fragment is
+// loaded once for the blocks whose lists contain it.  Every output block takes its terms in its own
+// list order, each term rounded to FP32 once as in k_mult_tc6, so the result is the same bits for
+// every G.
+template <int kG>
+__global__ void __launch_bounds__(128) k_mult_tc6g(TCArgs M) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= M.n_groups) return;
+  const int2 grp = M.groups[w];
+  int64_t p[kG], pe[kG];
+  int nx[kG];
+  double acc[kG][2][4];
+#pragma unroll
+  for (int b = 0; b < kG; ++b) {
+    if (b < grp.y) { p[b] = M.ptr[grp.x + b]; pe[b] = M.ptr[grp.x + b + 1]; }
+    else { p[b] = 0; pe[b] = 0; }
+    nx[b] = p[b] < pe[b] ? M.pairs[p[b]].x : INT_MAX;
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) acc[b][h][r] = 0.0;
+  }
+  while (true) {
+    int kc = INT_MAX;
+#pragma unroll
+    for (int b = 0; b < kG; ++b) kc = min(kc, nx[b]);
+    if (kc == INT_MAX) break;
+    const uint4 ah = __ldg(M.xa_hi + (int64_t)kc * 32 + lane);
+    const uint4 am = __ldg(M.xa_mid + (int64_t)kc * 32 + lane);
+    const uint4 al = __ldg(M.xa_lo + (int64_t)kc * 32 + lane);
+#pragma unroll
+    for (int b = 0; b < kG; ++b) {
+      if (nx[b] == kc) {
+        const int y = M.pairs[p[b]].y;
+        const uint4 bh = __ldg(M.bb_hi + (int64_t)y * 32 + lane);
+        const uint4 bm = __ldg(M.bb_mid + (int64_t)y * 32 + lane);
+        const uint4 bl = __ldg(M.bb_lo + (int64_t)y * 32 + lane);
+        float t[2][4];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) t[h][r] = 0.f;
+        mma_bf16(t[0], ah, bl.x, bl.y);
+        mma_bf16(t[0], al, bh.x, bh.y);
+        mma_bf16(t[0], am, bm.x, bm.y);
+        mma_bf16(t[0], ah, bm.x, bm.y);
+        mma_bf16(t[0], am, bh.x, bh.y);
+        mma_bf16(t[0], ah, bh.x, bh.y);
+        mma_bf16(t[1], ah, bl.z, bl.w);
+        mma_bf16(t[1], al, bh.z, bh.w);
+        mma_bf16(t[1], am, bm.z, bm.w);
+        mma_bf16(t[1], ah, bm.z, bm.w);
+        mma_bf16(t[1], am, bh.z, bh.w);
+        mma_bf16(t[1], ah, bh.z, bh.w);
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int r = 0; r < 4; ++r) acc[b][h][r] += (double)t[h][r];
+        ++p[b];
+        nx[b] = p[b] < pe[b] ? M.pairs[p[b]].x : INT_MAX;
+      }
+    }
+  }
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int b = 0; b < kG; ++b) {
+    if (b < grp.y) {
+      const int q = grp.x + b;
+      const int ndr = M.prim_nsf[M.o_row[q]], ndc = M.cover_nsf[M.o_cover[q]];
+      double* O = M.out + M.o_elem[q];
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          int row = g + ((r & 2) ? 8 : 0), col = 8 * h + 2 * t4 + (r & 1);
+          if (row < ndr && col < ndc) O[row + ndr * col] = acc[b][h][r];
+        }
+    }
+  }
+}
+
 }  // namespace
 
 // A-role (first operand) or B-role fragments of a whole range, hi and lo parts (1 KB per block)
-void to_fragments(System& S, int r, const double* src, int role_b, int trans, uint4* hi, uint4* lo) {
+// (and the middle parts of the three-part split when `mid` is given)
+void to_fragments(System& S, int r, const double* src, int role_b, int trans, uint4* hi, uint4* lo, uint4* mid) {
   RangeIndex& R = *S.ranges[r];
   if (R.nnz == 0) return;
   int64_t threads = (int64_t)R.nnz * 32;
   k_to_frag<<<(int)((threads + 255) / 256), 256, 0, S.stream>>>(R.nnz, R.nb_elem.p, R.nb_row.p, R.nb_cover.p,
                                                                 S.dg.prim_nsf.p, S.dg.cover_nsf.p, src, role_b, trans,
-                                                                hi, lo);
+                                                                hi, lo, mid);
   S.launches++;
   CQ_CUDA(cudaGetLastError());
 }
 
-static FragBuf& frag_buffer(System& S, int r, int slot) {
+static FragBuf& frag_buffer(System& S, int r, int slot, bool three = false) {
   FragBuf& f = S.frags[std::make_pair(r, slot)];
   size_t need = (size_t)std::max(S.ranges[r]->nnz, 1) * 32;
   if (f.hi.n < need) { f.hi.alloc(need, S.stream); f.lo.alloc(need, S.stream); }
+  if (three && f.mid.n < need) f.mid.alloc(need, S.stream);
   return f;
 }
 
@@ -245,9 +421,77 @@ static void mat_mult_mma_sync(System& S, MixedPlan& MP, int mult_type, int ra, i
   double* out = mult_type == 1 ? c : a;
   FragBuf& fx = frag_buffer(S, rx, 0);
   FragBuf& fb = frag_buffer(S, rb, 1);
-  to_fragments(S, rx, x, 0, 0, fx.hi.p, fx.lo.p);
-  to_fragments(S, rb, b, 1, mult_type == 2 ? 1 : 0, fb.hi.p, fb.lo.p);
+  to_fragments(S, rx, x, 0, 0, fx.hi.p, fx.lo.p, nullptr);
+  to_fragments(S, rb, b, 1, mult_type == 2 ? 1 : 0, fb.hi.p, fb.lo.p, nullptr);
   launch_mult_tc(S, MP, fx.hi.p, fx.lo.p, fb.hi.p, fb.lo.p, out);
+}
+
+static void ensure_groups(System& S, MixedPlan& MP, int gi);
+static void launch_tc6_g(System& S, MixedPlan& MP, TCArgs M, int gi);
+
+// three-part split products (one output block per warp)
+static void mat_mult_split6(System& S, MixedPlan& MP, int mult_type, int ra, int rb, int rc, double* a,
+                            const double* b, double* c) {
+  int rx = mult_type == 1 ? ra : rc;
+  const double* x = mult_type == 1 ? a : c;
+  double* out = mult_type == 1 ? c : a;
+  FragBuf& fx = frag_buffer(S, rx, 0, true);
+  FragBuf& fb = frag_buffer(S, rb, 1, true);
+  to_fragments(S, rx, x, 0, 0, fx.hi.p, fx.lo.p, fx.mid.p);
+  to_fragments(S, rb, b, 1, mult_type == 2 ? 1 : 0, fb.hi.p, fb.lo.p, fb.mid.p);
+  RangeIndex& O = *S.ranges[MP.out_range];
+  if (O.nnz == 0) return;
+  ensure_groups(S, MP, 0);
+  TCArgs M;
+  M.ptr = MP.ptr;
+  M.pairs = MP.pairs;
+  M.xa_hi = fx.hi.p; M.xa_lo = fx.lo.p; M.xa_mid = fx.mid.p;
+  M.bb_hi = fb.hi.p; M.bb_lo = fb.lo.p; M.bb_mid = fb.mid.p;
+  M.o_row = O.nb_row.p; M.o_cover = O.nb_cover.p; M.o_elem = O.nb_elem.p;
+  M.prim_nsf = S.dg.prim_nsf.p; M.cover_nsf = S.dg.cover_nsf.p;
+  M.out = out;
+  if (MP.tuned_g6 < 0) {
+    // autotuner: groups of 1, 2 and 4 output blocks (the same bits), as for the two-part kernel
+    cudaEvent_t e0, e1;
+    CQ_CUDA(cudaEventCreate(&e0));
+    CQ_CUDA(cudaEventCreate(&e1));
+    float best[3] = {1e30f, 1e30f, 1e30f};
+    for (int gi = 0; gi < 3; ++gi) launch_tc6_g(S, MP, M, gi);
+    for (int round = 0; round < 3; ++round)
+      for (int gi = 0; gi < 3; ++gi) {
+        CQ_CUDA(cudaEventRecord(e0, S.stream));
+        launch_tc6_g(S, MP, M, gi);
+        CQ_CUDA(cudaEventRecord(e1, S.stream));
+        CQ_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best[gi] = std::min(best[gi], ms);
+      }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int pick = 0;
+    for (int gi = 1; gi < 3; ++gi)
+      if (best[gi] < 0.95f * best[pick]) pick = gi;
+    for (int gi = 0; gi < 3; ++gi) MP.tune_ms6[gi] = best[gi];
+    MP.tuned_g6 = pick;
+  }
+  const int forced = S.split_group == 1 ? 0 : S.split_group == 2 ? 1 : S.split_group == 4 ? 2 : -1;
+  launch_tc6_g(S, MP, M, forced >= 0 ? forced : MP.tuned_g6);
+}
+
+// gi = 0: one output block per warp with prefetch; 1, 2: groups of 2 and 4 blocks of one row
+static void launch_tc6_g(System& S, MixedPlan& MP, TCArgs M, int gi) {
+  static const int kGi[3] = {0, 1, 2};   // index into the group sizes 1, 2, 4, 8
+  ensure_groups(S, MP, kGi[gi]);
+  M.groups = MP.groups[kGi[gi]].p;
+  M.n_groups = MP.n_groups[kGi[gi]];
+  if (M.n_groups == 0) return;
+  const int grid = (M.n_groups * 32 + 127) / 128;
+  if (gi == 0) k_mult_tc6<<<grid, 128, 0, S.stream>>>(M);
+  else if (gi == 1) k_mult_tc6g<2><<<grid, 128, 0, S.stream>>>(M);
+  else k_mult_tc6g<4><<<grid, 128, 0, S.stream>>>(M);
+  S.launches++;
+  CQ_CUDA(cudaGetLastError());
 }
 
 // Kernel choice of a split-precision product: the system's setting, or (setting -1) a fixed rule on
@@ -259,8 +503,13 @@ static void mat_mult_mma_sync(System& S, MixedPlan& MP, int mult_type, int ra, i
 // the tiles were faster for the product with fraction 0.114 (31.1 against 29.3) and slower below.
 constexpr double kTileMinFill = 0.11;
 
-void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c) {
+void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c,
+                    int parts) {
   MixedPlan& MP = get_mixed_plan(S, mult_type, ra, rb, rc);
+  if (parts == 3) {
+    mat_mult_split6(S, MP, mult_type, ra, rb, rc, a, b, c);
+    return;
+  }
   const bool tiles_ok = umma_usable(S, mult_type, ra, rb, rc);
   int k = S.mixed_kernel;
   if (k == 0 && !tiles_ok) k = 1;
@@ -278,7 +527,7 @@ void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a,
   else mat_mult_mma_sync(S, MP, mult_type, ra, rb, rc, a, b, c);
 }
 
-static void launch_tc_g(System& S, MixedPlan& MP, TCArgs M, int gi) {
+static void ensure_groups(System& S, MixedPlan& MP, int gi) {
   static const int kGs[4] = {1, 2, 4, 8};
   if (MP.n_groups[gi] < 0) {
     // groups of up to G consecutive output blocks of one row
@@ -291,6 +540,10 @@ static void launch_tc_g(System& S, MixedPlan& MP, TCArgs M, int gi) {
     MP.n_groups[gi] = (int)grp.size();
     MP.groups[gi].upload(grp, S.stream);
   }
+}
+
+static void launch_tc_g(System& S, MixedPlan& MP, TCArgs M, int gi) {
+  ensure_groups(S, MP, gi);
   M.groups = MP.groups[gi].p;
   M.n_groups = MP.n_groups[gi];
   if (M.n_groups == 0) return;
@@ -310,6 +563,7 @@ void launch_mult_tc(System& S, MixedPlan& MP, const uint4* xa_hi, const uint4* x
   M.ptr = MP.ptr;
   M.pairs = MP.pairs;
   M.xa_hi = xa_hi; M.xa_lo = xa_lo; M.bb_hi = bb_hi; M.bb_lo = bb_lo;
+  M.xa_mid = nullptr; M.bb_mid = nullptr;
   M.o_row = O.nb_row.p; M.o_cover = O.nb_cover.p; M.o_elem = O.nb_elem.p;
   M.prim_nsf = S.dg.prim_nsf.p; M.cover_nsf = S.dg.cover_nsf.p;
   M.out = out;
@@ -341,7 +595,8 @@ void launch_mult_tc(System& S, MixedPlan& MP, const uint4* xa_hi, const uint4* x
     for (int gi = 0; gi < 4; ++gi) MP.tune_ms[gi] = best[gi];
     MP.tuned_g = pick;
   }
-  launch_tc_g(S, MP, M, MP.tuned_g);
+  const int forced = S.split_group == 1 ? 0 : S.split_group == 2 ? 1 : S.split_group == 4 ? 2 : S.split_group == 8 ? 3 : -1;
+  launch_tc_g(S, MP, M, forced >= 0 ? forced : MP.tuned_g);
 }
 
 }  // namespace cqb

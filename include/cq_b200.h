@@ -100,13 +100,18 @@ int cq_export_radius(cq_system* sys, int r, double* out, int64_t cap, int64_t* n
  *   CQ_PREC_FP64_FMA (0): FP64 with fused multiply-add;
  *   CQ_PREC_BF16X3 (2): blocks padded to 16 x 16 and split v = hi + lo in bf16,
  *     hi.hi + hi.lo + lo.hi on the tensor cores with FP32 accumulation, stored
- *     back as FP64 (about 16 significant bits per product term).
+ *     back as FP64 (about 16 significant bits per product term);
+ *   CQ_PREC_BF16X6 (3): blocks padded to 16 x 16 and split v = hi + mid + lo in
+ *     bf16, six products per block pair (hi.hi, hi.mid, mid.hi, hi.lo, lo.hi,
+ *     mid.mid) on the tensor cores (mma.sync), each pair's product rounded once
+ *     to FP32 and the pairs summed in FP64 (about 22 significant bits per term).
  * The pair lists of the product are built on the first call and cached.  Work
  * is enqueued on the system's stream; the call returns without synchronising.
  */
 #define CQ_PREC_FP64_FMA 0
 #define CQ_PREC_FP64 1
 #define CQ_PREC_BF16X3 2
+#define CQ_PREC_BF16X6 3
 int cq_mat_mult(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a_dev, const double* b_dev,
                 double* c_dev, int precision);
 
@@ -275,7 +280,8 @@ int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out)
  * spins in cudaStreamSynchronize (default, lowest latency for one solver). */
 #define CQ_OPT_MULT_VARIANT 1
 #define CQ_OPT_BLOCKING_SYNC 2
-/* CQ_OPT_MIXED_KERNEL: kernel of the CQ_PREC_BF16X3 products.  -1 (default) = chosen per product
+/* CQ_OPT_MIXED_KERNEL: kernel of the CQ_PREC_BF16X3 products (CQ_PREC_BF16X6 products always run on
+ * mma.sync: the tcgen05 tiles accumulate a whole contraction in FP32).  -1 (default) = chosen per product
  * by a fixed rule (the tiles where at least 11 % of their issued tensor work is useful), so a product
  * always gives the same bits; 0 = dense 128 x 128 tiles on the tcgen05 tensor cores with TMEM
  * accumulators, operands staged by bulk copies (every block size 4..16; other systems use 1);
@@ -286,6 +292,10 @@ int cq_generate_SH(cq_system* sys, int r, int which, uint64_t seed, double* out)
  * synchronises (cq_mat_mult_host, cq_synchronize, the chain's waits) returns CQ_ERR_TIMEOUT; the
  * context stays usable and the product's output is not valid.  One product, then back to 0. */
 #define CQ_OPT_TEST_STALL 4
+/* CQ_OPT_SPLIT_GROUP: output blocks per warp of the mma.sync split-precision kernels.  -1 (default)
+ * = chosen per product by the autotuner; 1, 2, 4 (and 8, two-part split only) = that group size.
+ * Every group size gives the same bits (each output block sums its own terms in its own order). */
+#define CQ_OPT_SPLIT_GROUP 5
 int cq_system_set_option(cq_system* sys, int option, int value);
 
 /* ------------------------------------------------------------------------ */
@@ -311,11 +321,12 @@ typedef struct {
   int max_outer;           /* bound on FindMinDM outer passes (40); the reference loops until done, which a
                               residual stalled above `tolerance` never reaches: the solve then stops with
                               converged = 0 */
-  int mixed;               /* 1: cq_lnv_solve runs FindMinDM (McWeeny start included) with CQ_PREC_BF16X3
-                              products to `mixed_tolerance` (at most two passes, leaving at least one of
-                              `max_outer`), then continues from that L with FP64 products to `tolerance`;
+  int mixed;               /* 1: cq_lnv_solve runs FindMinDM (McWeeny start included) with split-precision
+                              products (split_parts) to `mixed_tolerance` (at most mixed_max_outer passes),
+                              then continues from that L with FP64 products to `tolerance`;
                               Hotelling, traces, line search and Pulay stay FP64 */
-  double mixed_tolerance;  /* residual at which the split-precision phase hands over to FP64 (1e-6) */
+  double mixed_tolerance;  /* residual at which the split-precision phase hands over to FP64; <= 0
+                              (default): max(tolerance, 1e-8) for split_parts 3, 1e-6 for split_parts 2 */
   int fp64_mcw_sweeps;     /* FP64 McWeeny purification sweeps of L between the two phases (0) */
   int graphs;              /* 1: each LNV_matrix_multiply call is captured once in a CUDA graph and replayed
                               (same results; default 1) */
@@ -324,6 +335,11 @@ typedef struct {
   int fp64_continue;       /* mixed form: 1 = FindMinDM continues in FP64 to `tolerance` (default);
                               0 = after the split-precision phase only the FP64 purification sweeps
                               (fp64_mcw_sweeps) and an FP64 evaluation of K, energy and electrons */
+  int split_parts;         /* mixed form: bf16 parts per value of the split-precision products,
+                              2 = CQ_PREC_BF16X3, 3 = CQ_PREC_BF16X6 (default) */
+  int mixed_max_outer;     /* mixed form: FindMinDM passes of the split-precision phase (always leaving
+                              at least one of max_outer to FP64); 0 (default) = 2 for split_parts 2,
+                              4 for split_parts 3 */
 } cq_lnv_params;
 
 typedef struct {
@@ -433,6 +449,16 @@ int cq_lnv_set_h_rebuild(cq_lnv* s, cq_h_rebuild_fn fn, void* user);
  * the new state.  Two chains that take the same steps log the same sequence, so the first
  * differing entry locates the first differing step. */
 int cq_lnv_reduction_log(cq_lnv* s, int enable, double* out, int64_t cap, int64_t* n);
+
+/* Iteration record of the last cq_lnv_solve (the reference's list of Pulay residuals and
+ * energies, PulayR / PulayE, DMMinModule.f90:289-294, with its per-iteration printout,
+ * DMMinModule.f90:539-541 and 1000-1002): one entry per earlyDM and lateDM iteration, five
+ * doubles each -- the residual g, the band energy 2 Tr(K H), the number of block products
+ * run by the solve so far, 1.0 if the iteration's products were split-precision (0.0 for
+ * FP64), and the host seconds since the solve started (taken once the residual has been read
+ * from the device).  *n = entries recorded (at most 65536), at most cap of them copied to out
+ * (5 * cap doubles).  Cleared when the next solve starts. */
+int cq_lnv_residual_history(cq_lnv* s, double* out, int64_t cap, int64_t* n);
 
 /* ------------------------------------------------------------------------ */
 /* Serving loop: continuous batching of independent density-matrix solves    */

@@ -100,9 +100,11 @@ def test_server_equals_direct_solver():
     assert (d["energy"], d["electrons"], d["n_products"]) == (r["energy"], r["electrons"], r["n_products"])
 
 
-def test_mixed_request_accuracy():
+@pytest.mark.parametrize("split_parts", [2, 3])
+def test_mixed_request_accuracy(split_parts):
     """Split-precision phase then FP64 continuation: same minimum as the FP64 solve within 1e-8 Ha/atom
-    (a 30-atom DZP cluster with L and T ranges beyond its diameter, so the minimum is well defined).
+    (a 30-atom DZP cluster with L and T ranges beyond its diameter, so the minimum is well defined), for
+    the two-part (hand-over at 1e-6) and three-part (hand-over at 1e-8) splits.
 
     Both solves stop at a residual of 1e-9: at the default 1e-7 two solves of the same problem from
     different starting points already differ by about 1e-7 Ha/atom, whatever their arithmetic."""
@@ -110,7 +112,7 @@ def test_mixed_request_accuracy():
     n = len(c)
     diam = float(np.max(np.linalg.norm(c[:, None] - c[None], axis=-1)))
     rg = (10.0, 12.0, diam + 1.0, diam + 1.0)
-    srv = cq_b200.Server(n_slots=2, tolerance=1e-9)
+    srv = cq_b200.Server(n_slots=2, tolerance=1e-9, split_parts=split_parts)
     fp = _run(srv, [(c, cell, 13, 2.0 * n, 7, False)], rg)[0]
     mx = _run(srv, [(c, cell, 13, 2.0 * n, 7, True)], rg)[0]
     srv.close()
@@ -122,10 +124,10 @@ def test_mixed_request_accuracy():
 
 def test_mixed_vs_fp64_truncated_dzp216():
     """The precision form on a config-3-shaped system: a truncated 216-atom DZP supercell (3x3x3 cells,
-    sigma 0.1 bohr, 13x13 blocks, S/H/L/T 10/12/16/10 bohr, 432 electrons), FP64 and mixed (split
-    products to residual 1e-6, then FP64) both to residual 1e-8 within 12 passes.  Measured on B200:
-    see the printed |dE| per atom; the bound here is the precision form's stated accuracy of 1e-7
-    Ha/atom against FP64 at that stop."""
+    sigma 0.1 bohr, 13x13 blocks, S/H/L/T 10/12/16/10 bohr, 432 electrons), FP64 and mixed (three-part
+    split products to residual 1e-8 within four passes, then FP64) both to residual 1e-8 within 12
+    passes.  Measured on B200: see the printed |dE| per atom; the bound here is the precision form's
+    stated accuracy of 1e-7 Ha/atom against FP64 at that stop."""
     c, cell = inputs.diamond_si(3, sigma=0.1, seed=77)
     srv = cq_b200.Server(n_slots=2, max_outer=12, tolerance=1e-8)
     ids = [srv.submit(c, cell, 13, 10.0, 12.0, 16.0, 10.0, 2.0 * len(c), seed=777, mixed=m) for m in (False, True)]

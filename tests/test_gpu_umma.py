@@ -20,32 +20,34 @@ pytestmark = pytest.mark.gpu
 TOL = 2.0 ** -14
 
 
-def _run(o, g, t, ia, ib, ic, bls_a, bls_b, bls_c, seed, kernel=0):
+def _run(o, g, t, ia, ib, ic, bls_a, bls_b, bls_c, seed, kernel=0, precision=None):
     """One product on both sides; returns (got, ref, sum |a||b| bound)."""
     import cq_b200
     g.set_mixed_kernel(kernel)
+    prec = cq_b200.PREC_BF16X3 if precision is None else precision
     b = inputs.random_blocks(bls_b, seed, inputs.TAG_RANDOM_B)
     if t == 1:
         a = inputs.random_blocks(bls_a, seed, inputs.TAG_RANDOM_A)
         ref = np.zeros(bls_c.length); o.mat_mult(1, ia, ib, ic, a, b, ref)
         bound = np.zeros(bls_c.length); o.mat_mult(1, ia, ib, ic, np.abs(a), np.abs(b), bound)
         got = np.full(bls_c.length, np.nan)
-        g.mat_mult_host(1, ia, ib, ic, a, b, got, precision=cq_b200.PREC_BF16X3)
+        g.mat_mult_host(1, ia, ib, ic, a, b, got, precision=prec)
     else:
         c = inputs.random_blocks(bls_c, seed + 1, inputs.TAG_RANDOM_A)
         ref = np.zeros(bls_a.length); o.mat_mult(2, ia, ib, ic, ref, b, c)
         bound = np.zeros(bls_a.length); o.mat_mult(2, ia, ib, ic, bound, np.abs(b), np.abs(c))
         got = np.full(bls_a.length, np.nan)
-        g.mat_mult_host(2, ia, ib, ic, got, b, c, precision=cq_b200.PREC_BF16X3)
+        g.mat_mult_host(2, ia, ib, ic, got, b, c, precision=prec)
     return got, ref, bound
 
 
-def _assert_bound(got, ref, bound):
+def _assert_bound(got, ref, bound, tol=TOL):
     assert not np.any(np.isnan(got)), "output blocks left unwritten"
     err = np.abs(got - ref)
     worst = np.max(err / np.maximum(bound, 1e-300))
-    assert np.all(err <= TOL * bound + 1e-300), "worst error / sum|a||b| = %.3g" % worst
+    assert np.all(err <= tol * bound + 1e-300), "worst error / sum|a||b| = %.3g" % worst
     assert err.max() > 0          # it really ran in reduced precision
+    return worst
 
 
 @pytest.fixture(scope="module")
@@ -143,3 +145,72 @@ def test_bounded_wait_reports_timeout_and_context_survives(cfg1):
     assert ei.value.code == cq_b200.CQ_ERR_TIMEOUT
     got, ref, bound = _run(o, g, 1, 0, 1, 2, bls[0], bls[1], bls[2], 82)
     _assert_bound(got, ref, bound)
+
+
+# Three-part split (BF16x6): v = hi + mid + lo, six products per block pair, each pair's 16 x 16 x 16
+# product rounded to FP32 once and the pairs summed in FP64.  The omitted products and split
+# remainders are below 2^-23 |a||b| per element product and the FP32 rounding of a pair's product
+# adds at most a few 2^-24 of its magnitude, so 2^-20 sum |a||b| bounds the error with margin.
+TOL6 = 2.0 ** -20
+
+
+@pytest.mark.parametrize("mult_type", [1, 2])
+def test_three_part_split_dzp_within_bound(cfg1, mult_type):
+    """216-atom Si, 13x13 blocks: the three-part split against the FP64 default kernel, and at least
+    2^6 times more accurate than the two-part split on the same product."""
+    import cq_b200
+    o, g, bls = cfg1
+    got6, ref, bound = _run(o, g, mult_type, 0, 1, 2, bls[0], bls[1], bls[2], 91 + mult_type,
+                            precision=cq_b200.PREC_BF16X6)
+    w6 = _assert_bound(got6, ref, bound, TOL6)
+    got3, _, _ = _run(o, g, mult_type, 0, 1, 2, bls[0], bls[1], bls[2], 91 + mult_type, kernel=1)
+    w3 = _assert_bound(got3, ref, bound)
+    print("worst error / sum|a||b|: three-part %.3g, two-part %.3g" % (w6, w3))
+    assert w6 * 64 < w3
+
+
+@pytest.mark.parametrize("prod", SZ_PRODUCTS[:3])
+def test_three_part_split_sz_within_bound(cfg2, prod):
+    """512-atom Si, 4x4 blocks (padded to 16 x 16), products of the LNV chain."""
+    import cq_b200
+    o, g, bls, idx = cfg2
+    t, ra, rb, rc = prod
+    got, ref, bound = _run(o, g, t, idx[ra], idx[rb], idx[rc], bls[ra], bls[rb], bls[rc], 93,
+                           precision=cq_b200.PREC_BF16X6)
+    _assert_bound(got, ref, bound, TOL6)
+
+
+def test_three_part_split_mixed_sizes_within_bound():
+    """Atoms with 4 and 13 orbitals in one system."""
+    import cq_b200
+    coords, cell = inputs.diamond_si(2, sigma=0.05, seed=21)
+    nsf = np.where(np.arange(len(coords)) % 3 == 0, 13, 4).astype(np.int32)
+    rc = [6.0, 8.0, 14.0]
+    o = OracleSystem(coords, cell, nsf, rc)
+    g = cq_b200.System(coords, cell, nsf, rc)
+    bls = [bm.oracle_blocklist(o, r, coords, cell) for r in range(3)]
+    for t in (1, 2):
+        got, ref, bound = _run(o, g, t, 0, 1, 2, bls[0], bls[1], bls[2], 95, precision=cq_b200.PREC_BF16X6)
+        _assert_bound(got, ref, bound, TOL6)
+
+
+@pytest.mark.parametrize("precision_name", ["PREC_BF16X3", "PREC_BF16X6"])
+def test_split_group_sizes_give_the_same_bits(cfg1, precision_name):
+    """The mma.sync split kernels with 1, 2, 4 (and 8) output blocks per warp: the same bits."""
+    import cq_b200
+    o, g, bls = cfg1
+    prec = getattr(cq_b200, precision_name)
+    sizes = [1, 2, 4, 8] if prec == cq_b200.PREC_BF16X3 else [1, 2, 4]
+    outs = []
+    try:
+        for gs in sizes:
+            g.set_split_group(gs)
+            for t in (1, 2):
+                got, _, _ = _run(o, g, t, 0, 1, 2, bls[0], bls[1], bls[2], 97, kernel=1, precision=prec)
+                outs.append((gs, t, got))
+    finally:
+        g.set_split_group(-1)
+    for t in (1, 2):
+        ref = [x for gs, tt, x in outs if tt == t]
+        for x in ref[1:]:
+            assert np.array_equal(x, ref[0])
