@@ -27,7 +27,7 @@ P = ctypes.POINTER
 # cq_h_rebuild_fn: (user, K_dev, H_dev, length, stream) -> status
 H_REBUILD_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_void_p, c_void_p, c_int64, c_void_p)
 # product arithmetic (cq_mat_mult precision)
-PREC_FP64_FMA, PREC_FP64, PREC_BF16X3, PREC_BF16X6 = 0, 1, 2, 3
+PREC_FP64_FMA, PREC_FP64, PREC_BF16X3, PREC_BF16X6, PREC_FP64_TC = 0, 1, 2, 3, 4
 
 
 class LNVParams(ctypes.Structure):
@@ -37,7 +37,7 @@ class LNVParams(ctypes.Structure):
                 ("invs_max_steps", c_int), ("invs_delta_tol", c_double), ("invs_tol", c_double), ("exact", c_int),
                 ("max_outer", c_int), ("mixed", c_int), ("mixed_tolerance", c_double), ("fp64_mcw_sweeps", c_int),
                 ("graphs", c_int), ("mixed_mcw", c_int), ("fp64_continue", c_int), ("split_parts", c_int),
-                ("mixed_max_outer", c_int)]
+                ("mixed_max_outer", c_int), ("fp64_tensor", c_int)]
 
 
 class LNVResult(ctypes.Structure):
@@ -234,7 +234,8 @@ class System:
 
     # ---- products and algebra on device memory ------------------------------
     def mat_mult(self, mult_type, ra, rb, rc, a, b, c, exact=True, precision=None):
-        """precision: PREC_FP64 (default kernel rounding), PREC_FP64_FMA, PREC_BF16X3 or PREC_BF16X6 (tensor cores, two- or three-part split)."""
+        """precision: PREC_FP64 (default kernel rounding), PREC_FP64_FMA, PREC_BF16X3 or PREC_BF16X6 (tensor cores,
+        two- or three-part split), PREC_FP64_TC (FP64 on the tensor cores)."""
         prec = int(bool(exact)) if precision is None else int(precision)
         check(lib().cq_mat_mult(self._h, mult_type, ra, rb, rc, _ptr(a), _ptr(b), _ptr(c), prec))
 

@@ -213,8 +213,8 @@ int cq_mat_mult(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a
     check_sys(sys); check_range(sys, ra); check_range(sys, rb); check_range(sys, rc);
     CQ_CHECK(a_dev && b_dev && c_dev, CQ_ERR_ARG, "null operand");
     ProductPlan& P = get_plan(sys->S, mult_type, ra, rb, rc);
-    CQ_CHECK(exact >= CQ_PREC_FP64_FMA && exact <= CQ_PREC_BF16X6, CQ_ERR_ARG, "unknown precision");
-    if (exact >= CQ_PREC_BF16X3)
+    CQ_CHECK(exact >= CQ_PREC_FP64_FMA && exact <= CQ_PREC_FP64_TC, CQ_ERR_ARG, "unknown precision");
+    if (exact == CQ_PREC_BF16X3 || exact == CQ_PREC_BF16X6)
       mat_mult_mixed(sys->S, mult_type, ra, rb, rc, a_dev, b_dev, c_dev, exact == CQ_PREC_BF16X6 ? 3 : 2);
     else launch_mat_mult(sys->S, P, a_dev, b_dev, c_dev, exact);
   });
@@ -274,7 +274,7 @@ int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, doub
   return guarded([&] {
     check_sys(sys); check_range(sys, ra); check_range(sys, rb); check_range(sys, rc);
     CQ_CHECK(a && b && c, CQ_ERR_ARG, "null operand");
-    CQ_CHECK(exact >= CQ_PREC_FP64_FMA && exact <= CQ_PREC_BF16X6, CQ_ERR_ARG, "unknown precision");
+    CQ_CHECK(exact >= CQ_PREC_FP64_FMA && exact <= CQ_PREC_FP64_TC, CQ_ERR_ARG, "unknown precision");
     System& S = sys->S;
     int64_t la = S.ranges[ra]->length, lb = S.ranges[rb]->length, lc = S.ranges[rc]->length;
     if (sys->ha.n < (size_t)std::max<int64_t>(la, 1)) sys->ha.alloc(std::max<int64_t>(la, 1), sys->S.stream);
@@ -284,7 +284,7 @@ int cq_mat_mult_host(cq_system* sys, int mult_type, int ra, int rb, int rc, doub
     if (mult_type == 1) CQ_CUDA(cudaMemcpyAsync(sys->ha.p, a, la * sizeof(double), cudaMemcpyHostToDevice, S.stream));
     CQ_CUDA(cudaMemcpyAsync(sys->hb.p, b, lb * sizeof(double), cudaMemcpyHostToDevice, S.stream));
     if (mult_type == 2) CQ_CUDA(cudaMemcpyAsync(sys->hc.p, c, lc * sizeof(double), cudaMemcpyHostToDevice, S.stream));
-    if (exact >= CQ_PREC_BF16X3)
+    if (exact == CQ_PREC_BF16X3 || exact == CQ_PREC_BF16X6)
       mat_mult_mixed(S, mult_type, ra, rb, rc, sys->ha.p, sys->hb.p, sys->hc.p, exact == CQ_PREC_BF16X6 ? 3 : 2);
     else launch_mat_mult(S, P, sys->ha.p, sys->hb.p, sys->hc.p, exact);
     if (mult_type == 1) CQ_CUDA(cudaMemcpyAsync(c, sys->hc.p, lc * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
@@ -746,12 +746,12 @@ int cq_matrix_product_id(cq_system* sys, int mult_type, int ida, int idb, int id
   return guarded([&] {
     check_sys(sys);
     CQ_CHECK(mult_type == 1 || mult_type == 2, CQ_ERR_ARG, "mult_type must be 1 or 2");
-    CQ_CHECK(precision >= CQ_PREC_FP64_FMA && precision <= CQ_PREC_BF16X6, CQ_ERR_ARG, "unknown precision");
+    CQ_CHECK(precision >= CQ_PREC_FP64_FMA && precision <= CQ_PREC_FP64_TC, CQ_ERR_ARG, "unknown precision");
     const int out = mult_type == 1 ? idc : ida;
     CQ_CHECK(out != (mult_type == 1 ? ida : idc) && out != idb, CQ_ERR_ARG, "the product's output must not be an input");
     BoundMatrix &A = bound(sys, ida), &B = bound(sys, idb), &C = bound(sys, idc);
     ProductPlan& P = get_plan(sys->S, mult_type, A.r, B.r, C.r);
-    if (precision >= CQ_PREC_BF16X3)
+    if (precision == CQ_PREC_BF16X3 || precision == CQ_PREC_BF16X6)
       mat_mult_mixed(sys->S, mult_type, A.r, B.r, C.r, A.dev.p, B.dev.p, C.dev.p, precision == CQ_PREC_BF16X6 ? 3 : 2);
     else launch_mat_mult(sys->S, P, A.dev.p, B.dev.p, C.dev.p, precision);
   });

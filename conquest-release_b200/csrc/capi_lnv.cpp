@@ -71,6 +71,7 @@ int cq_lnv_params_default(cq_lnv_params* p) {
   p->fp64_continue = 1;
   p->split_parts = 3;
   p->mixed_max_outer = 0;
+  p->fp64_tensor = 1;
   return CQ_OK;
 }
 
@@ -82,7 +83,8 @@ int cq_lnv_create(cq_system* sys, const int* ranges, double ne_spin, const cq_ln
     if (p) prm = *p;
     CQ_CHECK(prm.maxpulay >= 1 && prm.maxpulay <= 16, CQ_ERR_ARG, "maxpulay must be 1..16");
     CQ_CHECK(ne_spin > 0, CQ_ERR_ARG, "ne_spin must be positive");
-    CQ_CHECK(prm.split_parts == 2 || prm.split_parts == 3, CQ_ERR_ARG, "split_parts must be 2 or 3");
+    CQ_CHECK(prm.split_parts == 0 || prm.split_parts == 2 || prm.split_parts == 3, CQ_ERR_ARG,
+             "split_parts must be 0, 2 or 3");
     CQ_CHECK(prm.mixed_max_outer >= 0, CQ_ERR_ARG, "mixed_max_outer must be >= 0");
     auto s = std::make_unique<cq_lnv>();
     s->solver = std::make_unique<LNVSolver>(system_of(sys), ranges, ne_spin, prm);

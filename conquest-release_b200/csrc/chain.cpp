@@ -89,6 +89,9 @@ void LNVSolver::mult_dispatch(ProductPlan& P, double* a, const double* b, double
     stats.n_products_mixed++;
     stats.flops_mixed += P.flops;
     mat_mult_mixed(S, P.mult_type, P.ra, P.rb, P.rc, a, b, c, prm.split_parts);
+  } else if (prm.mixed && prm.fp64_tensor && S.max_nsf > 8) {
+    // the mixed form's FP64 products on the FP64 tensor cores (padded 16 x 16 blocks)
+    launch_mat_mult(S, P, a, b, c, kPrecFp64Tensor);
   } else if (S.batch_submit) {
     S.batch_submit(P, a, b, c, prm.exact);
   } else {
@@ -109,7 +112,7 @@ void LNVSolver::solve() {
   invert_S();                       // T = S^-1 in FP64 in both forms
   // no product of this system would run in split precision (mult_dispatch keeps blocks of 8 x 8
   // or less in FP64): the mixed form is the FP64 solve, in one phase
-  if (!prm.mixed || S.max_nsf <= 8) {
+  if (!prm.mixed || S.max_nsf <= 8 || prm.split_parts == 0) {
     find_min_dm(true);
     return;
   }

@@ -366,6 +366,9 @@ void launch_mult_tc(System& S, MixedPlan& MP, const uint4* xa_hi, const uint4* x
                     const uint4* bb_lo, double* out);
 // split-precision mat_mult with the roles of launch_mat_mult: tcgen05 tiles where every block size is
 // 4..128 (unless the system selects the per-block kernel), else the per-block mma.sync kernel
+// `exact` argument of launch_mat_mult: 1 = the reference kernel's separate multiply and add, 0 = fused
+// multiply-add, kPrecFp64Tensor = FP64 on the tensor cores (DMMA); the values of CQ_PREC_* in the C ABI
+constexpr int kPrecFp64Tensor = 4;
 // parts = 2: BF16x3 (tcgen05 tiles or mma.sync blocks by the fill rule); parts = 3: BF16x6 (mma.sync)
 void mat_mult_mixed(System& S, int mult_type, int ra, int rb, int rc, double* a, const double* b, double* c,
                     int parts = 2);

@@ -104,7 +104,11 @@ int cq_export_radius(cq_system* sys, int r, double* out, int64_t cap, int64_t* n
  *   CQ_PREC_BF16X6 (3): blocks padded to 16 x 16 and split v = hi + mid + lo in
  *     bf16, six products per block pair (hi.hi, hi.mid, mid.hi, hi.lo, lo.hi,
  *     mid.mid) on the tensor cores (mma.sync), each pair's product rounded once
- *     to FP32 and the pairs summed in FP64 (about 22 significant bits per term).
+ *     to FP32 and the pairs summed in FP64 (about 22 significant bits per term);
+ *   CQ_PREC_FP64_TC (4): FP64 on the tensor cores (mma.sync.m8n8k4.f64, blocks
+ *     padded to 16 x 16): each MMA chains its products as fused multiply-adds in
+ *     the terms' order, so the result has the bits of CQ_PREC_FP64_FMA (measured
+ *     on B200), which runs this way for blocks larger than 8 x 8.
  * The pair lists of the product are built on the first call and cached.  Work
  * is enqueued on the system's stream; the call returns without synchronising.
  */
@@ -112,6 +116,7 @@ int cq_export_radius(cq_system* sys, int r, double* out, int64_t cap, int64_t* n
 #define CQ_PREC_FP64 1
 #define CQ_PREC_BF16X3 2
 #define CQ_PREC_BF16X6 3
+#define CQ_PREC_FP64_TC 4
 int cq_mat_mult(cq_system* sys, int mult_type, int ra, int rb, int rc, double* a_dev, const double* b_dev,
                 double* c_dev, int precision);
 
@@ -336,10 +341,14 @@ typedef struct {
                               0 = after the split-precision phase only the FP64 purification sweeps
                               (fp64_mcw_sweeps) and an FP64 evaluation of K, energy and electrons */
   int split_parts;         /* mixed form: bf16 parts per value of the split-precision products,
-                              2 = CQ_PREC_BF16X3, 3 = CQ_PREC_BF16X6 (default) */
+                              2 = CQ_PREC_BF16X3, 3 = CQ_PREC_BF16X6 (default); 0 = no split-precision
+                              phase (with fp64_tensor: every product on the FP64 tensor cores) */
   int mixed_max_outer;     /* mixed form: FindMinDM passes of the split-precision phase (always leaving
                               at least one of max_outer to FP64); 0 (default) = 2 for split_parts 2,
                               4 for split_parts 3 */
+  int fp64_tensor;         /* mixed form: 1 (default) = its FP64 products of blocks larger than 8 x 8
+                              (McWeeny start, Hotelling, the FP64 continuation) run as CQ_PREC_FP64_TC,
+                              the bits of fused multiply-add FP64; 0 = as `exact` */
 } cq_lnv_params;
 
 typedef struct {
