@@ -992,7 +992,8 @@ void launch_mat_mult(System& S, ProductPlan& P, double* a, const double* b, doub
   // fused multiply-add products of blocks larger than 8 x 8 run on the FP64 tensor cores: an m8n8k4 MMA
   // chains its four products into the accumulator as fused multiply-adds in k order, so the bits are
   // those of the CUDA-core kernels (checked on B200), about three times faster on 13 x 13 blocks
-  if (exact == kPrecFp64Tensor || (exact == 0 && S.max_nsf > 8)) {
+  // (unless a CUDA-core variant is forced with CQ_OPT_MULT_VARIANT)
+  if (exact == kPrecFp64Tensor || (exact == 0 && S.max_nsf > 8 && S.mult_variant == kVariantAuto)) {
     const int grid = (M.n_out * 32 + 127) / 128;
     if (P.mult_type == 1) k_mult_dmma<1><<<grid, 128, 0, st>>>(M);
     else k_mult_dmma<2><<<grid, 128, 0, st>>>(M);

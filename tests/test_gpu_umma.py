@@ -265,9 +265,18 @@ def test_fp64_tensor_mixed_sizes_within_bound():
 def test_fp64_tensor_equals_fused_multiply_add_kernel(cfg1, mult_type):
     """Measured property of the B200 FP64 tensor cores: an m8n8k4 MMA sums its four products into the
     accumulator as a chain of fused multiply-adds in k order, so the DMMA product gives the bits of the
-    FP64 kernel with fused multiply-add (PREC_FP64_FMA), which takes the same terms in the same order."""
+    CUDA-core FP64 kernels with fused multiply-add (variants 4 and 0 forced), which take the same terms in
+    the same order."""
     import cq_b200
     o, g, bls = cfg1
     tc, _, _ = _run(o, g, mult_type, 0, 1, 2, bls[0], bls[1], bls[2], 107, precision=cq_b200.PREC_FP64_TC)
-    fma, _, _ = _run(o, g, mult_type, 0, 1, 2, bls[0], bls[1], bls[2], 107, precision=cq_b200.PREC_FP64_FMA)
-    assert np.array_equal(tc, fma)
+    outs = []
+    try:
+        for v in (4, 0):      # the CUDA-core kernels (register tiles; one lane per element)
+            g.set_mult_variant(v)
+            fma, _, _ = _run(o, g, mult_type, 0, 1, 2, bls[0], bls[1], bls[2], 107, precision=cq_b200.PREC_FP64_FMA)
+            outs.append(fma)
+    finally:
+        g.set_mult_variant(-1)
+    for fma in outs:
+        assert np.array_equal(tc, fma)
