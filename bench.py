@@ -369,12 +369,13 @@ def main():
     ap.add_argument("--no-mixed-sample", action="store_true",
                     help="skip the mixed-precision vs FP64 comparison on the bounded DZP sample")
     ap.add_argument("--workload", default="lnv512",
-                    choices=["lnv512", "batch", "serve", "mult216", "mult512", "mult216dzp", "mult4096"],
+                    choices=["lnv512", "batch", "serve", "mult216", "mult512", "mult216dzp", "mult4096", "forms216"],
                     help="lnv512: the plain FP64 512-atom solve (default); batch / serve: mixed-precision solves of "
                          "many systems on concurrent slots vs the FP64 path one at a time; mult216 / mult512 / "
                          "mult216dzp / mult4096: single block products (216-atom DZP C=A.B; the products of one LNV "
-                         "call on the 512-atom SZ, 216-atom DZP and 4096-atom DZP cells)")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3", "bf16x6"])
+                         "call on the 512-atom SZ, 216-atom DZP and 4096-atom DZP cells); forms216: one 216-atom "
+                         "DZP solve in each precision form")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fma", "bf16x3", "bf16x6", "fp64tc"])
     ap.add_argument("--variant", type=int, default=None, help="FP64 4x4 product kernel variant (-1 autotuned, 0..3, 5, 6)")
     ap.add_argument("--mixed-kernel", type=int, default=-1, choices=[-1, 0, 1],
                     help="split-precision products: -1 = chosen per product by the tile plan's useful fraction "
@@ -386,6 +387,10 @@ def main():
                          "all host cores; several minutes) and write the record as JSON to PATH")
     ap.add_argument("--one-solve", action="store_true",
                     help="run exactly one solve of the workload and print its result (for launch lists under ncu)")
+    ap.add_argument("--forms-cell", default="3,77,777", metavar="NCELL,SEED,SH_SEED",
+                    help="forms216: the periodic Si cell (cells per side, displacement seed, S/H generator seed)")
+    ap.add_argument("--forms", default=None, help="forms216: comma list of the forms to run (default all)")
+    ap.add_argument("--history-stride", type=int, default=4, help="forms216: every n-th iteration in the history")
     ap.add_argument("--requests", type=int, default=32)
     ap.add_argument("--nmin", type=int, default=64)
     ap.add_argument("--nmax", type=int, default=1000)
@@ -399,6 +404,8 @@ def main():
     ap.add_argument("--max-outer", type=int, default=None, help="batch/serve: FindMinDM pass limit per request")
     args = ap.parse_args()
     ws, rank, local = dist_env()
+    if args.workload == "forms216" and args.impl == "ours":
+        return forms_main(args)
     if args.workload in ("mult216", "mult512", "mult216dzp", "mult4096") and args.impl == "ours":
         if rank == 0:
             mult_main(args)
@@ -665,7 +672,8 @@ def mixed_vs_fp64(cq_b200, tol=None, max_outer=None, handover=None):
             "fp64_residual": a["residual"], "mixed_residual": b["residual"],
             "fp64_electrons": a["electrons"], "mixed_electrons": b["electrons"],
             "dE_per_atom_Ha": (b["energy"] - a["energy"]) / a["n_atoms"], "fp64_s": a["t_done"] - a["t_admit"],
-            "mixed_s": b["t_done"] - b["t_admit"]} for a, b in zip(fp, mx) if a["status"] == 0 and b["status"] == 0]
+            "mixed_s": b["t_done"] - b["t_admit"], "split_restart": b["split_restarts"]}
+           for a, b in zip(fp, mx) if a["status"] == 0 and b["status"] == 0]
     both = [abs(r["dE_per_atom_Ha"]) for r in per if r["fp64_converged"] and r["mixed_converged"]]
     return {"sample": "4 periodic DZP (13x13) Si supercells of 64 atoms; S/H/L/T 10/12/16/10 bohr; both arms stop at "
                       "residual %g (pass limit %d)" % (tol_used, mo_used),
@@ -741,12 +749,90 @@ def serve_main(args):
                          "mixed_s": b["t_done"] - b["t_admit"], "conv": [a["converged"], b["converged"]],
                          "dE_per_atom": (b["energy"] - a["energy"]) / a["n_atoms"],
                          "products": [a["n_products"], b["n_products"]],
-                         "flops": [a["flops"], b["flops"]], "flops_split_mixed": b["flops_mixed"]}
+                         "flops": [a["flops"], b["flops"]], "flops_split_mixed": b["flops_mixed"],
+                         "split_restart": b["split_restarts"]}
                         for a, b, q in zip(fp, mx, reqs)],
         "bytes_peak_max": max(r["bytes_peak"] for r in mx),
         "clocks": clk.summary(),
     }
     emit(line)
+
+
+# ----------------------------------------------------------------------------
+# precision forms of one DZP solve
+# ----------------------------------------------------------------------------
+FORMS = [("fp64", dict(exact=1)),
+         ("fp64_fma", dict(exact=0)),
+         ("fp64_tensor", dict(mixed=1, split_parts=0)),
+         ("bf16x6+fp64_tensor", dict(mixed=1)),
+         ("bf16x6+fp64", dict(mixed=1, fp64_tensor=0)),
+         ("bf16x3+fp64", dict(mixed=1, split_parts=2, fp64_tensor=0))]
+
+
+def forms_main(args):
+    """One 216-atom DZP solve (3x3x3 Si cells, sigma 0.1 bohr, seed 77; 13x13 blocks; S/H/L/T 10/12/16/10
+    bohr; 432 electrons; S and H from the device generators with seed 777) in each precision form: the
+    plain FP64 path, FP64 with fused multiply-add on the CUDA cores and on the FP64 tensor cores, and the
+    mixed forms.  Every solve stops at residual --tol (default 1e-8) within 16 passes; one untimed solve
+    of the plain and of the default mixed form first builds and tunes the plans."""
+    import torch
+    import cq_b200
+    from cq_b200 import inputs
+    torch.cuda.set_device(0)
+    tol = args.tol if args.tol is not None else 1e-8
+    ncell, cseed, shseed = (int(x) for x in args.forms_cell.split(","))
+    coords, cell = inputs.diamond_si(ncell, sigma=0.1, seed=cseed)
+    n = len(coords)
+    rng = cq_b200.lnv_ranges(10.0, 12.0, 16.0, 10.0)
+    ridx = {k: i for i, k in enumerate(rng)}
+    g = cq_b200.System(coords, cell, np.full(n, 13, np.int32), list(rng.values()))
+    dev = torch.device("cuda", 0)
+    S = torch.empty(g.length(ridx["S"]), dtype=torch.float64, device=dev)
+    H = torch.empty(g.length(ridx["H"]), dtype=torch.float64, device=dev)
+    g.generate_SH(ridx["S"], 0, shseed, S)
+    g.generate_SH(ridx["H"], 1, shseed, H)
+    torch.cuda.synchronize()
+
+    def solve(kw):
+        sol = cq_b200.LNV(g, ridx, float(n), tolerance=tol, max_outer=16, **kw)
+        sol.set_SH(S, H)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = sol.solve()
+        dt = time.perf_counter() - t0
+        h = sol.residual_history()
+        sol.close()
+        return r, dt, h
+
+    forms = [f for f in FORMS if not args.forms or f[0] in args.forms.split(",")]
+    for kw in (FORMS[0][1], FORMS[3][1]):
+        solve(kw)
+    out, ref = [], None
+    with ClockSampler(0) as clk:
+        for name, kw in forms:
+            r, dt, h = solve(kw)
+            if ref is None:
+                ref = r
+            split_rows = [x for x in h if x[3] == 1]
+            out.append({"form": name, "seconds": dt, "speedup_vs_fp64": None if not out else out[0]["seconds"] / dt,
+                        "energy": r["energy"], "dE_per_atom_vs_fp64": (r["energy"] - ref["energy"]) / n,
+                        "converged": r["converged"], "residual": r["residual"], "products": r["n_products"],
+                        "products_split": r["n_products_mixed"], "iterations": len(h),
+                        "seconds_to_first_iteration": float(h[0][4]) if len(h) else None,
+                        "split_phase_end": None if not split_rows else
+                        {"residual": float(split_rows[-1][0]), "seconds": float(split_rows[-1][4]),
+                         "products": int(split_rows[-1][2])},
+                        "history": [[float("%.3g" % x[0]), int(x[2]), int(x[3]), round(float(x[4]), 2)]
+                                    for x in h[::args.history_stride]]})
+    if out:
+        out[0]["speedup_vs_fp64"] = 1.0
+    emit({"metric": "one DZP LNV solve per precision form (seconds)", "value": out[-1]["seconds"], "unit": "s",
+          "n_gpus": 1, "higher_is_better": False, "dtype": "f64 / bf16x6+f64 / bf16x3+f64", "data": "synthetic",
+          "config": {"workload": "forms216", "system": "%d-atom Si DZP (13x13), %dx%dx%d cells, sigma 0.1, seed %d, "
+                                                     "S/H seed %d" % (n, ncell, ncell, ncell, cseed, shseed),
+                     "ranges_bohr": {"S": 10.0, "H": 12.0, "L": 16.0, "T": 10.0}, "electrons": 2 * n,
+                     "tolerance": tol, "max_outer": 16},
+          "forms": out, "clocks": clk.summary()})
 
 
 # ----------------------------------------------------------------------------
@@ -770,7 +856,7 @@ def mult_main(args):
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     prec = {"fp64": cq_b200.PREC_FP64, "fma": cq_b200.PREC_FP64_FMA, "bf16x3": cq_b200.PREC_BF16X3,
-            "bf16x6": cq_b200.PREC_BF16X6}[args.precision]
+            "bf16x6": cq_b200.PREC_BF16X6, "fp64tc": cq_b200.PREC_FP64_TC}[args.precision]
     if args.workload == "mult216":
         coords, cell = inputs.diamond_si(3, sigma=0.05, seed=1)
         n = len(coords)
@@ -833,7 +919,7 @@ def mult_main(args):
     tot_ms = sum(o["ms"] for o in out)
     emit({"metric": "block-mult TFLOP/s (%s)" % args.precision, "value": tot_fl / (tot_ms / 1e3) / 1e12,
           "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-          "dtype": {"fp64": "f64", "fma": "f64", "bf16x3": "bf16x3", "bf16x6": "bf16x6"}[args.precision],
+          "dtype": {"fp64": "f64", "fma": "f64", "bf16x3": "bf16x3", "bf16x6": "bf16x6", "fp64tc": "f64"}[args.precision],
           "data": "synthetic", "config": {"workload": args.workload, "system": desc, "variant": args.variant,
                                           "mixed_kernel": args.mixed_kernel,
                                           "l2": "flushed (256 MB write) before every timed launch"},

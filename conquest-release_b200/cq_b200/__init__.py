@@ -47,7 +47,7 @@ class LNVResult(ctypes.Structure):
                 ("inflexions", c_int), ("converged", c_int), ("outer_iters", c_int), ("graph_launches", c_int64),
                 ("n_products", c_int64),
                 ("flops", c_int64),
-                ("n_products_mixed", c_int64), ("flops_mixed", c_int64)]
+                ("n_products_mixed", c_int64), ("flops_mixed", c_int64), ("split_restarts", c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -609,7 +609,7 @@ class RequestResult(ctypes.Structure):
                 ("slot", c_int), ("energy", c_double), ("electrons", c_double), ("residual", c_double),
                 ("n_products", c_int64), ("flops", c_int64), ("n_products_mixed", c_int64), ("flops_mixed", c_int64),
                 ("t_arrival", c_double), ("t_admit", c_double), ("t_done", c_double), ("bytes_estimate", c_int64),
-                ("bytes_peak", c_int64), ("message", ctypes.c_char * 128)]
+                ("bytes_peak", c_int64), ("message", ctypes.c_char * 128), ("split_restarts", c_int)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_}

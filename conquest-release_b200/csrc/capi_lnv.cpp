@@ -33,6 +33,7 @@ static void fill_result(const LNVStats& st, cq_lnv_result* r) {
   r->flops = st.flops;
   r->n_products_mixed = st.n_products_mixed;
   r->flops_mixed = st.flops_mixed;
+  r->split_restarts = st.split_restarts;
 }
 
 static DMat* matrix_by_name(LNVSolver& L, const char* name) {

@@ -124,8 +124,9 @@ void LNVSolver::solve() {
   // hand-over residual: the three-part split carries the solve to the final tolerance (its products'
   // rounding, about 1e-7 of sum |a||b|, stalls the residual near 1e-8 on DZP Si), the two-part split
   // to 1e-6
-  prm.tolerance = prm.mixed_tolerance > 0 ? prm.mixed_tolerance
-                                          : (prm.split_parts == 3 ? std::max(tol, 1e-8) : 1e-6);
+  const double handover = prm.mixed_tolerance > 0 ? prm.mixed_tolerance
+                                                 : (prm.split_parts == 3 ? std::max(tol, 1e-8) : 1e-6);
+  prm.tolerance = handover;
   // the split phase gets a bounded number of passes and leaves at least one to the FP64 continuation:
   // where the split products' rounding keeps the residual above the hand-over (small dense clusters
   // with the two-part split), a stalled split phase must not use up the passes the FP64 phase needs
@@ -153,11 +154,17 @@ void LNVSolver::solve() {
     return;
   }
   stats.converged = 0;
-  // both phases share the pass limit of the FP64 solve (at least one FP64 pass)
+  // A split phase that ended far above its hand-over residual (more than 100 times) has stalled, and
+  // on small dense DZP systems its L can lie where FP64 FindMinDM no longer reaches the tolerance
+  // within the passes left (measured: 1e-3 Ha/atom from the FP64 solve): the FP64 phase then starts
+  // again from the McWeeny start with the whole pass limit.  Otherwise both phases share the pass
+  // limit of the FP64 solve (at least one FP64 pass) and FP64 continues from the split phase's L.
+  const bool restart = stats.last_residual > 100.0 * handover;
+  if (restart) stats.split_restarts++;
   const int max_outer = prm.max_outer;
-  prm.max_outer = std::max(1, max_outer - stats.outer_iters);
+  prm.max_outer = restart ? max_outer : std::max(1, max_outer - stats.outer_iters);
   try {
-    find_min_dm(false);
+    find_min_dm(restart);
   } catch (...) {
     prm.max_outer = max_outer;
     throw;

@@ -39,6 +39,7 @@ struct LNVStats {
   int64_t n_products = 0, flops = 0, n_reductions = 0, n_lnv = 0, n_products_mixed = 0, flops_mixed = 0;
   int mcw_sweeps = 0, early_iters = 0, late_iters = 0, ne_corrections = 0, inflexions = 0, converged = 0;
   int outer_iters = 0;
+  int split_restarts = 0;         // mixed form: FP64 phases started again from the McWeeny start
   int64_t graph_launches = 0;     // LNV calls run as CUDA graph launches
   double energy = 0, electrons = 0, last_energy = 0, last_residual = 0, invs_omega = 0;
   double mubar = 0, lambda = 0, hmin = 0, hmax = 0;

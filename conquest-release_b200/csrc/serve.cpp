@@ -359,6 +359,7 @@ class Server {
       res.flops = s.flops;
       res.n_products_mixed = s.n_products_mixed;
       res.flops_mixed = s.flops_mixed;
+      res.split_restarts = s.split_restarts;
     });
     if (res.status != CQ_OK) {
       std::strncpy(res.message, cq_last_error(), sizeof(res.message) - 1);

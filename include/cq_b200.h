@@ -363,6 +363,9 @@ typedef struct {
   int64_t flops;           /* algorithmic flops of those products (2 sum nd_i nd_j nd_k) */
   int64_t n_products_mixed;/* of which with split-precision tensor-core arithmetic */
   int64_t flops_mixed;
+  int split_restarts;      /* mixed form: 1 if the split-precision phase stalled more than 100 times
+                              above its hand-over residual and the FP64 phase started again from the
+                              McWeeny start */
 } cq_lnv_result;
 
 int cq_lnv_params_default(cq_lnv_params* p);
@@ -522,6 +525,7 @@ typedef struct {
   int64_t bytes_estimate;  /* admission estimate */
   int64_t bytes_peak;      /* device bytes the solve actually held at its peak */
   char message[128];       /* error message when status != CQ_OK */
+  int split_restarts;      /* cq_lnv_result.split_restarts of the solve */
 } cq_request_result;
 
 typedef struct cq_server cq_server;
