@@ -160,7 +160,16 @@ void LNVSolver::solve() {
   // again from the McWeeny start with the whole pass limit.  Otherwise both phases share the pass
   // limit of the FP64 solve (at least one FP64 pass) and FP64 continues from the split phase's L.
   const bool restart = stats.last_residual > 100.0 * handover;
-  if (restart) stats.split_restarts++;
+  if (restart) {
+    // the FP64 solve from the beginning: the chain's matrices cleared and T = S^-1 again, as at the
+    // start of solve() (measured: a FindMinDM restart that kept the split phase's T and chain
+    // matrices did not converge where the FP64 solve from the beginning does)
+    stats.split_restarts++;
+    for (DMat* m : {&L, &T, &Ttran, &LS, &SL, &K, &phi})
+      CQ_CUDA(cudaMemsetAsync(m->p, 0, sizeof(double) * std::max<int64_t>(m->n, 1), S.stream));
+    delta_e = 0.0;
+    invert_S();
+  }
   const int max_outer = prm.max_outer;
   prm.max_outer = restart ? max_outer : std::max(1, max_outer - stats.outer_iters);
   try {
