@@ -942,7 +942,9 @@ struct KernArgs {
   const Halo* ahalo; const Halo* chalo; const Trans* at;
 };
 
-// m_kern_max, default kernel (multiply_kernel_default.f90:132-224)
+// m_kern_max, default kernel (multiply_kernel_default.f90:132-224); FMA = true: the same terms in
+// the same order, each multiply-add fused (std::fma, one rounding)
+template <bool FMA = false>
 static void m_kern_max_default(const KernArgs& K) {
   const Halo& ah = *K.ahalo; const Halo& ch = *K.chalo; const Trans& at = *K.at;
   vector<int> jbnab2ch(64);
@@ -977,7 +979,8 @@ static void m_kern_max_default(const KernArgs& K) {
               for (int n1 = 1; n1 <= nd1; ++n1) {
                 int naaddr = nabeg + nd3 * (n1 - 1);
                 for (int n3 = 1; n3 <= nd3; ++n3)
-                  K.c[ncaddr + n1 - 1] = K.c[ncaddr + n1 - 1] + K.a[naaddr + n3 - 1] * K.b[nbaddr + n3 - 1];
+                  K.c[ncaddr + n1 - 1] = FMA ? std::fma(K.a[naaddr + n3 - 1], K.b[nbaddr + n3 - 1], K.c[ncaddr + n1 - 1])
+                                             : K.c[ncaddr + n1 - 1] + K.a[naaddr + n3 - 1] * K.b[nbaddr + n3 - 1];
               }
             }
           }
@@ -989,7 +992,8 @@ static void m_kern_max_default(const KernArgs& K) {
   }
 }
 
-// m_kern_min, default kernel (multiply_kernel_default.f90:325-412)
+// m_kern_min, default kernel (multiply_kernel_default.f90:325-412); FMA as for m_kern_max_default
+template <bool FMA = false>
 static void m_kern_min_default(const KernArgs& K) {
   const Halo& ah = *K.ahalo; const Halo& ch = *K.chalo; const Trans& at = *K.at;
   vector<int> jbnab2ch(64);
@@ -1024,7 +1028,8 @@ static void m_kern_min_default(const KernArgs& K) {
               for (int n1 = 1; n1 <= nd1; ++n1) {
                 int naaddr = nabeg + nd3 * (n1 - 1);
                 for (int n3 = 1; n3 <= nd3; ++n3)
-                  K.a[naaddr + n3 - 1] = K.a[naaddr + n3 - 1] + K.c[ncaddr + n1 - 1] * K.b[nbaddr + n3 - 1];
+                  K.a[naaddr + n3 - 1] = FMA ? std::fma(K.c[ncaddr + n1 - 1], K.b[nbaddr + n3 - 1], K.a[naaddr + n3 - 1])
+                                             : K.a[naaddr + n3 - 1] + K.c[ncaddr + n1 - 1] * K.b[nbaddr + n3 - 1];
               }
             }
           }
@@ -1244,7 +1249,8 @@ static void m_kern_min_ompgemm(const KernArgs& K) {
 }
 
 // mat_mult (multiply_module.f90:115-359), one process: prefetch = Mquest_get_local
-// kernel: 0 = default, 1 = ompGemm
+// kernel: 0 = default, 1 = ompGemm, 2 = ompDoii, 3 = count only, 4 = default order with fused
+// multiply-add
 static void mat_mult(System& s, int mult_type, int ra, int rb, int rc, double* a0, int lena, const double* b0, int lenb,
                      double* c0, int lenc, int kernel, int nthreads) {
   Range& A = s.ranges[ra]; Range& B = s.ranges[rb]; Range& C = s.ranges[rc];
@@ -1310,11 +1316,12 @@ static void mat_mult(System& s, int mult_type, int ra, int rb, int rc, double* a
     K.ahalo = &A.halo; K.chalo = &C.halo; K.at = &A.trans;
     return K;
   };
-  if (kernel == 0 || kernel == 3) {
+  if (kernel == 0 || kernel == 3 || kernel == 4) {
     for (int kpart = 1; kpart <= np_in_halo; ++kpart) {
       prefetch_part(kpart);
       KernArgs K = make_args(kpart, A.halo.lab_hcover[kpart]);
       if (kernel == 3) m_kern_count(K);
+      else if (kernel == 4) { if (mult_type == 1) m_kern_max_default<true>(K); else m_kern_min_default<true>(K); }
       else if (mult_type == 1) m_kern_max_default(K);
       else m_kern_min_default(K);
     }

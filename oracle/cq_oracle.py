@@ -159,10 +159,12 @@ class OracleSystem:
 
         type 1: a = A (range ra), b = B (range rb), c = C (range rc) is overwritten.
         type 2: a = output (range ra) accumulates, b = B (range rb), c = input (range rc).
+        kernel: "default" (multiply_kernel_default.f90, separate multiply and add), "ompGemm", "ompDoii",
+        or "default_fma" (the default kernel's terms in its order, each multiply-add fused).
         """
         for arr in (a, b, c):
             assert arr.dtype == np.float64 and arr.flags.c_contiguous
-        k = {"default": 0, "ompGemm": 1, "ompDoii": 2}[kernel]
+        k = {"default": 0, "ompGemm": 1, "ompDoii": 2, "default_fma": 4}[kernel]
         st = self._lib.orc_mat_mult(self._h, mult_type, ra, rb, rc, _dp(a), a.size, _dp(b), b.size, _dp(c), c.size,
                                     k, int(nthreads))
         if st != 0:

@@ -191,3 +191,27 @@ def test_tiny_cells_match_image_arithmetic(case):
     o.mat_mult(2, 0, 1, 2, out, b, cin)
     ck2 = bm.kat_type2(bls[0], bls[1], b, bls[2], cin)
     assert np.abs(out - ck2).max() < 1e-13 * np.abs(ck2).max()
+
+
+def test_default_kernel_with_fused_multiply_add(dzp_cfg1):
+    """The oracle's default kernel with each multiply-add fused ("default_fma", the order of the GPU's
+    fused-multiply-add and FP64 tensor-core products): the same sums to FP64 rounding (a few 2^-53 of
+    sum |a||b|), and really different roundings (not the same bits as the separate multiply and add)."""
+    coords, cell, o = dzp_cfg1
+    blA, blB, blC = [bm.oracle_blocklist(o, r, coords, cell) for r in range(3)]
+    a = inputs.random_blocks(blA, 111, inputs.TAG_RANDOM_A)
+    b = inputs.random_blocks(blB, 111, inputs.TAG_RANDOM_B)
+    for t in (1, 2):
+        if t == 1:
+            c0 = np.zeros(blC.length); c1 = np.zeros(blC.length); bound = np.zeros(blC.length)
+            o.mat_mult(1, 0, 1, 2, a, b, c0)
+            o.mat_mult(1, 0, 1, 2, a, b, c1, kernel="default_fma")
+            o.mat_mult(1, 0, 1, 2, np.abs(a), np.abs(b), bound)
+        else:
+            cin = inputs.random_blocks(blC, 112, inputs.TAG_RANDOM_A)
+            c0 = np.zeros(blA.length); c1 = np.zeros(blA.length); bound = np.zeros(blA.length)
+            o.mat_mult(2, 0, 1, 2, c0, b, cin)
+            o.mat_mult(2, 0, 1, 2, c1, b, cin, kernel="default_fma")
+            o.mat_mult(2, 0, 1, 2, bound, np.abs(b), np.abs(cin))
+        assert np.all(np.abs(c1 - c0) <= 1e-14 * bound)
+        assert not np.array_equal(c1, c0)
